@@ -1,0 +1,673 @@
+// C ABI of libesb: argument checking and launches of the kernel entry points,
+// and the Reconstructor (buffers, cuFFT plans, CTF slab loops, SART driver
+// loop, sub-volume back-projection).
+#include <cufft.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "esb_device.cuh"
+#include "esb_internal.h"
+
+namespace esb {
+
+cudaError_t launch_march(const KConst& c, const void* vol, int vt, float* proj, float* dist, size_t pitchE, int x0,
+                         int y0, int x1, int y1, cudaStream_t st);
+cudaError_t launch_slicer(const KConst& c, const void* vol, int vt, float* proj, size_t pitchE, float tmin, float tmax,
+                          int x0, int y0, int x1, int y1, cudaStream_t st);
+cudaError_t launch_travlen(const KConst& c, float* dist, size_t pitchE, int x0, int y0, int x1, int y1, cudaStream_t st);
+cudaError_t launch_bp(const KConst& c, void* vol, int vt, const float* img, int pw, int ph, size_t pitchE, float lambda,
+                      int os, float distMin, float distMax, int linear, cudaStream_t st);
+cudaError_t launch_compare(int pw, int ph, size_t pitchE, const float* real, float* virt, const float* dist,
+                           float realLength, float4 cut, float4 dim, float scale, cudaStream_t st);
+cudaError_t launch_crop_border(int pw, int ph, size_t pitchE, float* img, float2 cut, float2 dim, const int* p,
+                               cudaStream_t st);
+cudaError_t launch_make_square(int pw, int ph, size_t strideE, const float* in, int maxsize, float* out, int bx, int by,
+                               int mirrorY, int fillZero, cudaStream_t st);
+cudaError_t launch_crop_to_square(int pw, int ph, size_t pitchE, float* img, int apply_crop, float2 cut, float2 dim,
+                                  const int* p, int maxsize, float* sq, int bx, int by, cudaStream_t st);
+cudaError_t launch_square_to_image(const float* sq, int maxsize, size_t shift, float inv_norm, int pw, int ph,
+                                   size_t pitchE, float* out, float* accum, int apply_crop, float2 cut, float2 dim,
+                                   const int* p, cudaStream_t st);
+CtfConst make_ctf_const(int n, float cs_mm, float voltage_kv, float amp_contrast, float pixel_size_nm);
+cudaError_t launch_ctf(float* spec, int n, const CtfConst& k, float d0_nm, float d1_nm, float angle_deg, int applyForFP,
+                       int phaseFlip, float wiener, float4 beta, cudaStream_t st);
+cudaError_t launch_wbp_weighting(float* spec, int n, float psi_deg, int fm, cudaStream_t st);
+cudaError_t launch_fourier_filter(float* spec, int n, float lp, float hp, float lps, float hps, cudaStream_t st);
+cudaError_t launch_dose_weighting(float* spec, int n, float dose, float pixelsize, cudaStream_t st);
+cudaError_t launch_convert(const void* vol, int vt, long n, float* out, float sign, cudaStream_t st);
+cudaError_t launch_store(const float* in, long n, void* vol, int vt, cudaStream_t st);
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+static int cuda_fail(cudaError_t e, const char* where) {
+  return fail(ESB_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace esb
+
+using namespace esb;
+
+#define ESB_CK(call, where)                       \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+  } while (0)
+
+#define ESB_FFT(call, where)                                                         \
+  do {                                                                               \
+    cufftResult r_ = (call);                                                         \
+    if (r_ != CUFFT_SUCCESS)                                                         \
+      return fail(ESB_ERR_CUFFT, std::string(where) + ": cuFFT error " + std::to_string((int)r_)); \
+  } while (0)
+
+static inline cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
+static inline bool valid_vt(int vt) { return vt == ESB_VOXEL_F32 || vt == ESB_VOXEL_F16 || vt == ESB_VOXEL_BF16; }
+
+static int check_image(int pw, int ph, size_t pitch, const char* where) {
+  if (pw <= 0 || ph <= 0) return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": image size must be positive");
+  if (pitch < (size_t)pw * sizeof(float) || pitch % sizeof(float) != 0)
+    return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": pitch must be a multiple of 4 and >= width*4");
+  return ESB_OK;
+}
+
+static int check_constants(const esb_constants* c, const char* where) {
+  if (!c) return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": constants are NULL");
+  for (int k = 0; k < 3; ++k)
+    if (!(c->volume_dim[k] >= 1.0f) || c->volume_dim[k] != floorf(c->volume_dim[k]))
+      return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": volume_dim must be positive integers");
+  return ESB_OK;
+}
+
+extern "C" {
+
+const char* esb_last_error(void) { return g_last_error.c_str(); }
+int esb_version(void) { return 100; }
+
+int esb_fp(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj, float* dist,
+           size_t pitch, int roi_x0, int roi_y0, int roi_x1, int roi_y1, void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_fp")) || (r = check_image(proj_x, proj_y, pitch, "esb_fp"))) return r;
+  if (!vol || !proj || !dist || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_fp: invalid argument");
+  roi_x0 = roi_x0 < 0 ? 0 : roi_x0;
+  roi_y0 = roi_y0 < 0 ? 0 : roi_y0;
+  roi_x1 = roi_x1 > proj_x ? proj_x : roi_x1;
+  roi_y1 = roi_y1 > proj_y ? proj_y : roi_y1;
+  ESB_CK(launch_march(to_kconst(*c), vol, voxel_type, proj, dist, pitch / 4, roi_x0, roi_y0, roi_x1, roi_y1,
+                      as_stream(stream)), "esb_fp");
+  return ok();
+}
+
+int esb_fp_slicer(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj,
+                  size_t pitch, float tmin, float tmax, int roi_x0, int roi_y0, int roi_x1, int roi_y1, void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_fp_slicer")) || (r = check_image(proj_x, proj_y, pitch, "esb_fp_slicer"))) return r;
+  if (!vol || !proj || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_fp_slicer: invalid argument");
+  roi_x0 = roi_x0 < 0 ? 0 : roi_x0;
+  roi_y0 = roi_y0 < 0 ? 0 : roi_y0;
+  roi_x1 = roi_x1 > proj_x ? proj_x : roi_x1;
+  roi_y1 = roi_y1 > proj_y ? proj_y : roi_y1;
+  ESB_CK(launch_slicer(to_kconst(*c), vol, voxel_type, proj, pitch / 4, tmin, tmax, roi_x0, roi_y0, roi_x1, roi_y1,
+                       as_stream(stream)), "esb_fp_slicer");
+  return ok();
+}
+
+int esb_vol_traversal_length(const esb_constants* c, int proj_x, int proj_y, float* dist, size_t pitch, int roi_x0,
+                             int roi_y0, int roi_x1, int roi_y1, void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_vol_traversal_length")) ||
+      (r = check_image(proj_x, proj_y, pitch, "esb_vol_traversal_length")))
+    return r;
+  if (!dist) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_vol_traversal_length: dist is NULL");
+  roi_x0 = roi_x0 < 0 ? 0 : roi_x0;
+  roi_y0 = roi_y0 < 0 ? 0 : roi_y0;
+  roi_x1 = roi_x1 > proj_x ? proj_x : roi_x1;
+  roi_y1 = roi_y1 > proj_y ? proj_y : roi_y1;
+  ESB_CK(launch_travlen(to_kconst(*c), dist, pitch / 4, roi_x0, roi_y0, roi_x1, roi_y1, as_stream(stream)),
+         "esb_vol_traversal_length");
+  return ok();
+}
+
+int esb_compare(int proj_x, int proj_y, size_t pitch, const float* real, float* virt, const float* dist,
+                float real_length, const float crop[4], const float crop_dim[4], float proj_val_scale, void* stream) {
+  int r;
+  if ((r = check_image(proj_x, proj_y, pitch, "esb_compare"))) return r;
+  if (!real || !virt || !dist || !crop || !crop_dim) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_compare: NULL argument");
+  ESB_CK(launch_compare(proj_x, proj_y, pitch / 4, real, virt, dist, real_length,
+                        make_float4(crop[0], crop[1], crop[2], crop[3]),
+                        make_float4(crop_dim[0], crop_dim[1], crop_dim[2], crop_dim[3]), proj_val_scale,
+                        as_stream(stream)), "esb_compare");
+  return ok();
+}
+
+int esb_crop_border(int proj_x, int proj_y, size_t pitch, float* img, const float cut_length[2],
+                    const float dim_length[2], const int p[8], void* stream) {
+  int r;
+  if ((r = check_image(proj_x, proj_y, pitch, "esb_crop_border"))) return r;
+  if (!img || !cut_length || !dim_length || !p) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_crop_border: NULL argument");
+  ESB_CK(launch_crop_border(proj_x, proj_y, pitch / 4, img, make_float2(cut_length[0], cut_length[1]),
+                            make_float2(dim_length[0], dim_length[1]), p, as_stream(stream)), "esb_crop_border");
+  return ok();
+}
+
+int esb_bp(const esb_constants* c, void* vol, int voxel_type, int proj_x, int proj_y, const float* img, size_t pitch,
+           float lambda, int oversampling, float dist_min, float dist_max, int linear_filter, void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_bp")) || (r = check_image(proj_x, proj_y, pitch, "esb_bp"))) return r;
+  if (!vol || !img || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_bp: invalid argument");
+  if (oversampling < 1) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_bp: oversampling must be >= 1");
+  if (4 * c->volume_dim_x_quarter > (int)c->volume_dim[0])
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_bp: volume_dim_x_quarter exceeds volume_dim.x / 4");
+  ESB_CK(launch_bp(to_kconst(*c), vol, voxel_type, img, proj_x, proj_y, pitch / 4, lambda, oversampling, dist_min,
+                   dist_max, linear_filter, as_stream(stream)), "esb_bp");
+  return ok();
+}
+
+int esb_make_square(int proj_x, int proj_y, size_t pitch, const float* in, int maxsize, float* out, int border_x,
+                    int border_y, int mirror_y, int fill_zero, void* stream) {
+  int r;
+  if ((r = check_image(proj_x, proj_y, pitch, "esb_make_square"))) return r;
+  if (!in || !out || maxsize <= 0) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_make_square: invalid argument");
+  if (!fill_zero && (maxsize - border_x > 2 * proj_x || maxsize - border_y > 2 * proj_y || border_x > proj_x ||
+                     border_y > proj_y))
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_make_square: mirror padding wider than the image");
+  ESB_CK(launch_make_square(proj_x, proj_y, pitch / 4, in, maxsize, out, border_x, border_y, mirror_y, fill_zero,
+                            as_stream(stream)), "esb_make_square");
+  return ok();
+}
+
+int esb_ctf(float* spectrum, int n, float defocus_min_nm, float defocus_max_nm, float angle_deg, int apply_for_fp,
+            int phase_flip_only, float wiener_noise_level, const float beta_fac[4], float cs_mm, float voltage_kv,
+            float amp_contrast, float pixel_size_nm, void* stream) {
+  if (!spectrum || n <= 1 || !beta_fac || pixel_size_nm <= 0)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_ctf: invalid argument");
+  CtfConst k = make_ctf_const(n, cs_mm, voltage_kv, amp_contrast, pixel_size_nm);
+  ESB_CK(launch_ctf(spectrum, n, k, defocus_min_nm, defocus_max_nm, angle_deg, apply_for_fp, phase_flip_only,
+                    wiener_noise_level, make_float4(beta_fac[0], beta_fac[1], beta_fac[2], beta_fac[3]),
+                    as_stream(stream)), "esb_ctf");
+  return ok();
+}
+
+int esb_wbp_weighting(float* spectrum, int n, float psi_deg, int filter, void* stream) {
+  if (!spectrum || n <= 1 || filter < 0 || filter > 4)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_wbp_weighting: invalid argument");
+  ESB_CK(launch_wbp_weighting(spectrum, n, psi_deg, filter, as_stream(stream)), "esb_wbp_weighting");
+  return ok();
+}
+
+int esb_fourier_filter(float* spectrum, int n, float lp, float hp, float lps, float hps, void* stream) {
+  if (!spectrum || n <= 1) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_fourier_filter: invalid argument");
+  ESB_CK(launch_fourier_filter(spectrum, n, lp, hp, lps, hps, as_stream(stream)), "esb_fourier_filter");
+  return ok();
+}
+
+int esb_dose_weighting(float* spectrum, int n, float dose, float pixel_size_a, void* stream) {
+  if (!spectrum || n <= 1 || pixel_size_a <= 0) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_dose_weighting: invalid argument");
+  ESB_CK(launch_dose_weighting(spectrum, n, dose, pixel_size_a, as_stream(stream)), "esb_dose_weighting");
+  return ok();
+}
+
+int esb_convert_volume(const void* vol, int voxel_type, long n_voxels, float* out, int negate, void* stream) {
+  if (!vol || !out || n_voxels < 0 || !valid_vt(voxel_type))
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_convert_volume: invalid argument");
+  if (n_voxels == 0) return ok();
+  ESB_CK(launch_convert(vol, voxel_type, n_voxels, out, negate ? -1.0f : 1.0f, as_stream(stream)), "esb_convert_volume");
+  return ok();
+}
+
+int esb_store_volume(const float* in, long n_voxels, void* vol, int voxel_type, void* stream) {
+  if (!vol || !in || n_voxels < 0 || !valid_vt(voxel_type))
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_store_volume: invalid argument");
+  if (n_voxels == 0) return ok();
+  ESB_CK(launch_store(in, n_voxels, vol, voxel_type, as_stream(stream)), "esb_store_volume");
+  return ok();
+}
+
+}  // extern "C"
+
+// ===================================================================== Reconstructor
+
+// Pool of event pairs for one timing phase.
+struct PhaseTimer {
+  std::vector<cudaEvent_t> start, stop;
+  size_t used = 0;
+  cudaError_t begin(cudaStream_t s) {
+    if (used == start.size()) {
+      cudaEvent_t a, b;
+      cudaError_t e = cudaEventCreate(&a);
+      if (e != cudaSuccess) return e;
+      e = cudaEventCreate(&b);
+      if (e != cudaSuccess) return e;
+      start.push_back(a);
+      stop.push_back(b);
+    }
+    return cudaEventRecord(start[used], s);
+  }
+  cudaError_t end(cudaStream_t s) { return cudaEventRecord(stop[used++], s); }
+  void destroy() {
+    for (auto e : start) cudaEventDestroy(e);
+    for (auto e : stop) cudaEventDestroy(e);
+    start.clear();
+    stop.clear();
+    used = 0;
+  }
+};
+
+struct esb_reconstructor {
+  esb_recon_config cfg;
+  std::vector<esb_proj_geom> geoms;
+  std::vector<float> tilt;
+  std::vector<float> defocus;  // [n][3]: min nm, max nm, astigmatism angle deg
+  float aniso[9], anisoInv[9];
+  int N = 0;
+  int borderX = 0, borderY = 0;
+  size_t squareShift = 0;
+  float *proj_d = nullptr, *dist_d = nullptr, *real_d = nullptr;
+  float* square_d = nullptr;
+  float* fft_d = nullptr;
+  std::vector<float*> sirt_d;  // residual images of one ordered subset
+  bool plans = false;
+  cufftHandle r2c = 0, c2r = 0;
+  cudaStream_t stream = nullptr;
+  CtfConst ctfk;
+  bool timing = false;
+  PhaseTimer timers[4];
+};
+
+// Brackets a phase of launches with events when timing is enabled.
+struct PhaseScope {
+  esb_reconstructor* r;
+  int phase;
+  PhaseScope(esb_reconstructor* r_, int p) : r(r_), phase(p) {
+    if (r->timing) r->timers[phase].begin(r->stream);
+  }
+  ~PhaseScope() {
+    if (r->timing) r->timers[phase].end(r->stream);
+  }
+};
+
+static int rec_alloc(esb_reconstructor* r) {
+  const size_t img = (size_t)r->cfg.proj_x * r->cfg.proj_y * sizeof(float);
+  ESB_CK(cudaMalloc(&r->proj_d, img), "esb_reconstructor_create");
+  ESB_CK(cudaMalloc(&r->dist_d, img), "esb_reconstructor_create");
+  ESB_CK(cudaMalloc(&r->real_d, img), "esb_reconstructor_create");
+  ESB_CK(cudaMemset(r->proj_d, 0, img), "esb_reconstructor_create");
+  ESB_CK(cudaMemset(r->dist_d, 0, img), "esb_reconstructor_create");
+  if (r->cfg.ctf_mode) {
+    const int N = r->N;
+    ESB_CK(cudaMalloc(&r->square_d, (size_t)N * N * sizeof(float)), "esb_reconstructor_create");
+    ESB_CK(cudaMalloc(&r->fft_d, (size_t)(N / 2 + 1) * N * 2 * sizeof(float)), "esb_reconstructor_create");
+    ESB_FFT(cufftPlan2d(&r->r2c, N, N, CUFFT_R2C), "esb_reconstructor_create");
+    ESB_FFT(cufftPlan2d(&r->c2r, N, N, CUFFT_C2R), "esb_reconstructor_create");
+    r->plans = true;
+  }
+  return ESB_OK;
+}
+
+static void rec_free(esb_reconstructor* r) {
+  cudaFree(r->proj_d);
+  cudaFree(r->dist_d);
+  cudaFree(r->real_d);
+  cudaFree(r->square_d);
+  cudaFree(r->fft_d);
+  for (float* p : r->sirt_d) cudaFree(p);
+  r->sirt_d.clear();
+  if (r->plans) {
+    cufftDestroy(r->r2c);
+    cufftDestroy(r->c2r);
+  }
+  for (auto& t : r->timers) t.destroy();
+}
+
+extern "C" {
+
+int esb_reconstructor_create(const esb_recon_config* cfg, const esb_proj_geom* geoms, const float* tilt_deg,
+                             const float* defocus, const float mag_aniso[9], const float mag_aniso_inv[9],
+                             esb_reconstructor** out) {
+  if (!cfg || !geoms || !tilt_deg || !out)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_create: NULL argument");
+  if (cfg->proj_x <= 0 || cfg->proj_y <= 0 || cfg->n_proj <= 0 || cfg->oversampling < 1)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_create: invalid sizes");
+  if (cfg->ctf_mode && (!defocus || cfg->pixel_size_nm <= 0 || cfg->ctf_slice_thickness_nm <= 0))
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_create: CTF mode needs defocus, pixel size and slab thickness");
+  esb_reconstructor* r = new esb_reconstructor();
+  r->cfg = *cfg;
+  r->geoms.assign(geoms, geoms + cfg->n_proj);
+  r->tilt.assign(tilt_deg, tilt_deg + cfg->n_proj);
+  if (defocus) r->defocus.assign(defocus, defocus + 3 * (size_t)cfg->n_proj);
+  static const float ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  memcpy(r->aniso, mag_aniso ? mag_aniso : ident, sizeof(r->aniso));
+  memcpy(r->anisoInv, mag_aniso_inv ? mag_aniso_inv : ident, sizeof(r->anisoInv));
+  // Reconstructor::Reconstructor (Reconstructor.cpp:340-347): square image
+  // of the larger side, image centred in it.
+  r->N = cfg->proj_x > cfg->proj_y ? cfg->proj_x : cfg->proj_y;
+  size_t shx = (r->N - cfg->proj_x) / 2, shy = (size_t)((r->N - cfg->proj_y) / 2) * r->N;
+  r->squareShift = shx + shy;
+  r->borderX = (r->N - cfg->proj_x) / 2;
+  r->borderY = (r->N - cfg->proj_y) / 2;
+  if (cfg->ctf_mode) r->ctfk = make_ctf_const(r->N, cfg->cs_mm, cfg->voltage_kv, cfg->amp_contrast, cfg->pixel_size_nm);
+  int rc = rec_alloc(r);
+  if (rc != ESB_OK) {
+    std::string msg = esb_last_error();
+    rec_free(r);
+    delete r;
+    return fail(rc, msg);
+  }
+  *out = r;
+  return ok();
+}
+
+int esb_reconstructor_destroy(esb_reconstructor* rec) {
+  if (!rec) return ok();
+  rec_free(rec);
+  delete rec;
+  return ok();
+}
+
+int esb_reconstructor_set_stream(esb_reconstructor* rec, void* stream) {
+  if (!rec) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_set_stream: NULL reconstructor");
+  rec->stream = (cudaStream_t)stream;
+  if (rec->plans) {
+    ESB_FFT(cufftSetStream(rec->r2c, rec->stream), "esb_reconstructor_set_stream");
+    ESB_FFT(cufftSetStream(rec->c2r, rec->stream), "esb_reconstructor_set_stream");
+  }
+  return ok();
+}
+
+int esb_reconstructor_buffers(esb_reconstructor* rec, float** proj_d, float** dist_d, float** real_d) {
+  if (!rec) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_buffers: NULL reconstructor");
+  if (proj_d) *proj_d = rec->proj_d;
+  if (dist_d) *dist_d = rec->dist_d;
+  if (real_d) *real_d = rec->real_d;
+  return ok();
+}
+
+int esb_reconstructor_enable_timing(esb_reconstructor* rec, int enable) {
+  if (!rec) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_enable_timing: NULL reconstructor");
+  rec->timing = enable != 0;
+  for (auto& t : rec->timers) t.used = 0;
+  return ok();
+}
+
+int esb_reconstructor_timing(esb_reconstructor* rec, double out_ms[4], int counts[4]) {
+  if (!rec || !out_ms || !counts) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_timing: NULL argument");
+  ESB_CK(cudaStreamSynchronize(rec->stream), "esb_reconstructor_timing");
+  for (int p = 0; p < 4; ++p) {
+    double sum = 0;
+    PhaseTimer& t = rec->timers[p];
+    for (size_t i = 0; i < t.used; ++i) {
+      float ms = 0;
+      ESB_CK(cudaEventElapsedTime(&ms, t.start[i], t.stop[i]), "esb_reconstructor_timing");
+      sum += ms;
+    }
+    out_ms[p] = sum;
+    counts[p] = (int)t.used;
+    t.used = 0;
+  }
+  return ok();
+}
+
+int esb_rec_reset_projections(esb_reconstructor* r) {
+  if (!r) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_reset_projections: NULL reconstructor");
+  PhaseScope ps(r, 3);
+  const size_t img = (size_t)r->cfg.proj_x * r->cfg.proj_y * sizeof(float);
+  ESB_CK(cudaMemsetAsync(r->proj_d, 0, img, r->stream), "esb_rec_reset_projections");
+  ESB_CK(cudaMemsetAsync(r->dist_d, 0, img, r->stream), "esb_rec_reset_projections");
+  return ok();
+}
+
+}  // extern "C"
+
+static int rec_check(esb_reconstructor* r, const esb_vol_geom* vg, int index, const char* where) {
+  if (!r || !vg) return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": NULL argument");
+  if (index < 0 || index >= r->cfg.n_proj) return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": index out of range");
+  return ESB_OK;
+}
+
+static KConst rec_const(esb_reconstructor* r, const esb_proj_geom& g, const esb_vol_geom& vg, int for_bp) {
+  esb_constants c;
+  esb_set_constant_values(&g, &vg, r->aniso, r->anisoInv, for_bp, &c);
+  return to_kconst(c);
+}
+
+// CTF chain of one slab on `img` (W x H): optional in-place crop, pad to the
+// N x N square, R2C, CTF (FP or Wiener BP), C2R, scale 1/N^2, crop, and write
+// to `out` and/or accumulate into `accum` (Reconstructor.cpp:559-583, 952-965).
+static int rec_ctf_chain(esb_reconstructor* r, float* img, int crop_in, const int* p_in, int index, float dmin,
+                         float dmax, int for_fp, float* out, float* accum, int crop_out, const int* p_out) {
+  const esb_recon_config& cf = r->cfg;
+  const int W = cf.proj_x, H = cf.proj_y, N = r->N;
+  PhaseScope ps(r, 2);
+  float2 cut = make_float2(cf.cut_length[0], cf.cut_length[1]);
+  float2 dim = make_float2(cf.dim_length[0], cf.dim_length[1]);
+  ESB_CK(launch_crop_to_square(W, H, W, img, crop_in, cut, dim, p_in, N, r->square_d, r->borderX, r->borderY, r->stream),
+         "ctf chain");
+  ESB_FFT(cufftExecR2C(r->r2c, (cufftReal*)r->square_d, (cufftComplex*)r->fft_d), "ctf chain R2C");
+  float4 beta = make_float4(cf.ctf_beta_fac[0], cf.ctf_beta_fac[1], cf.ctf_beta_fac[2], cf.ctf_beta_fac[3]);
+  ESB_CK(launch_ctf(r->fft_d, N, r->ctfk, dmin, dmax, r->defocus[3 * index + 2], for_fp, cf.phase_flip_only,
+                    cf.wiener_noise_level, beta, r->stream), "ctf chain");
+  ESB_FFT(cufftExecC2R(r->c2r, (cufftComplex*)r->fft_d, (cufftReal*)r->square_d), "ctf chain C2R");
+  ESB_CK(launch_square_to_image(r->square_d, N, r->squareShift, 1.0f / ((float)N * (float)N), W, H, W, out, accum,
+                                crop_out, cut, dim, p_out, r->stream), "ctf chain");
+  return ESB_OK;
+}
+
+extern "C" {
+
+int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, const void* vol, int voxel_type, int index,
+                               int volume_is_empty) {
+  int rc;
+  if ((rc = rec_check(r, vg, index, "esb_rec_forward_projection"))) return rc;
+  if (!vol || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_forward_projection: invalid volume");
+  const esb_recon_config& cf = r->cfg;
+  const int W = cf.proj_x, H = cf.proj_y;
+  KConst c = rec_const(r, r->geoms[index], *vg, 0);
+  if (volume_is_empty) {  // Reconstructor.cpp:465-470 / 622-627
+    PhaseScope ps(r, 0);
+    ESB_CK(launch_travlen(c, r->dist_d, W, 0, 0, W, H, r->stream), "esb_rec_forward_projection");
+    return ok();
+  }
+  if (!cf.ctf_mode) {  // ForwardProjectionNoCTF (Reconstructor.cpp:429-438)
+    PhaseScope ps(r, 0);
+    ESB_CK(launch_march(c, vol, voxel_type, r->proj_d, r->dist_d, W, 0, 0, W, H, r->stream), "esb_rec_forward_projection");
+    return ok();
+  }
+  // ForwardProjectionCTF (Reconstructor.cpp:496-590)
+  float t_in, t_out;
+  esb_defocus_distances(&r->geoms[index], vg, W, H, &t_in, &t_out);
+  const float step = cf.ctf_slice_thickness_nm / cf.pixel_size_nm;
+  const int full[8] = {0, H - 1, W - 1, H - 1, 0, 0, W - 1, 0};  // pA, pB, pC, pD (Reconstructor.cpp:559-566)
+  for (float ray = t_in; ray < t_out; ray += step) {
+    float dmin, dmax;
+    esb_defocus_min_max(ray, r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index], cf.add_tilt_angle,
+                        cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2], cf.ignore_z_shift_for_ctf,
+                        cf.switch_ctf_direction, &dmin, &dmax);
+    {
+      PhaseScope ps(r, 3);
+      ESB_CK(cudaMemsetAsync(r->dist_d, 0, (size_t)W * H * sizeof(float), r->stream), "esb_rec_forward_projection");
+    }
+    {
+      PhaseScope ps(r, 0);
+      ESB_CK(launch_slicer(c, vol, voxel_type, r->dist_d, W, ray, ray + step, 0, 0, W, H, r->stream),
+             "esb_rec_forward_projection");
+    }
+    if ((rc = rec_ctf_chain(r, r->dist_d, 1, full, index, dmin, dmax, 1, nullptr, r->proj_d, 1, full))) return rc;
+  }
+  {
+    PhaseScope ps(r, 3);
+    ESB_CK(cudaMemsetAsync(r->dist_d, 0, (size_t)W * H * sizeof(float), r->stream), "esb_rec_forward_projection");
+  }
+  PhaseScope ps(r, 0);
+  ESB_CK(launch_travlen(c, r->dist_d, W, 0, 0, W, H, r->stream), "esb_rec_forward_projection");
+  return ok();
+}
+
+int esb_rec_compare(esb_reconstructor* r, const esb_vol_geom* vg, const float* real, int index) {
+  int rc;
+  if ((rc = rec_check(r, vg, index, "esb_rec_compare"))) return rc;
+  if (!real) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_compare: real is NULL");
+  const esb_recon_config& cf = r->cfg;
+  // Reconstructor::Compare (Reconstructor.cpp:1386-1405)
+  const float DIST = -10000.0f;
+  float zdir = r->geoms[index].proj_norm[2];
+  float zmin = vg->full_bbox_min[2], zmax = vg->full_bbox_max[2];
+  float len = fabsf((DIST - zmin) / zdir - (DIST - zmax) / zdir);
+  PhaseScope ps(r, 3);
+  ESB_CK(launch_compare(cf.proj_x, cf.proj_y, cf.proj_x, real, r->proj_d, r->dist_d, len,
+                        make_float4(cf.crop[0], cf.crop[1], cf.crop[2], cf.crop[3]),
+                        make_float4(cf.crop_dim[0], cf.crop_dim[1], cf.crop_dim[2], cf.crop_dim[3]),
+                        cf.projection_scale_factor, r->stream), "esb_rec_compare");
+  return ok();
+}
+
+}  // extern "C"
+
+// BackProjection of image `img` (Reconstructor.cpp:871-887 and 920-969).
+static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type, int index,
+                                  float sirt_count, float* img) {
+  const esb_recon_config& cf = r->cfg;
+  const int W = cf.proj_x, H = cf.proj_y;
+  int p[8];
+  esb_compute_hit_points(&r->geoms[index], vg, p);
+  KConst c = rec_const(r, r->geoms[index], *vg, 1);
+  const float lambda = cf.lambda / sirt_count;
+  if (!cf.ctf_mode) {
+    {
+      PhaseScope ps(r, 3);
+      ESB_CK(launch_crop_border(W, H, W, img, make_float2(cf.cut_length[0], cf.cut_length[1]),
+                                make_float2(cf.dim_length[0], cf.dim_length[1]), p, r->stream), "back projection");
+    }
+    PhaseScope ps(r, 1);
+    ESB_CK(launch_bp(c, vol, voxel_type, img, W, H, W, lambda, cf.oversampling, 0.0f, 9999999999999.0f, 0, r->stream),
+           "back projection");
+    return ESB_OK;
+  }
+  float t_in, t_out;
+  esb_defocus_distances(&r->geoms[index], vg, W, H, &t_in, &t_out);
+  const float step = cf.ctf_slice_thickness_nm / cf.pixel_size_nm;
+  int rc;
+  for (float ray = t_in; ray < t_out; ray += step) {
+    float dmin, dmax;
+    esb_defocus_min_max(ray, r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index], cf.add_tilt_angle,
+                        cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2], cf.ignore_z_shift_for_ctf,
+                        cf.switch_ctf_direction, &dmin, &dmax);
+    // cropBorder(proj_d) is re-applied to the residual on every slab (:954)
+    if ((rc = rec_ctf_chain(r, img, 1, p, index, dmin, dmax, 0, r->dist_d, nullptr, 1, p))) return rc;
+    PhaseScope ps(r, 1);
+    ESB_CK(launch_bp(c, vol, voxel_type, r->dist_d, W, H, W, lambda, cf.oversampling, ray, ray + step, 1, r->stream),
+           "back projection");
+  }
+  return ESB_OK;
+}
+
+extern "C" {
+
+int esb_rec_back_projection(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type, int index,
+                            float sirt_count) {
+  int rc;
+  if ((rc = rec_check(r, vg, index, "esb_rec_back_projection"))) return rc;
+  if (!vol || !valid_vt(voxel_type) || !(sirt_count > 0))
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_back_projection: invalid argument");
+  return rec_back_project_image(r, vg, vol, voxel_type, index, sirt_count, r->proj_d);
+}
+
+int esb_sart_run(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type, const float* projections,
+                 const int* index_list, int proj_count, int iterations, int sirt_count, int* volume_is_empty) {
+  if (!r || !vg || !vol || !projections || !index_list || !volume_is_empty || !valid_vt(voxel_type))
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_sart_run: NULL argument");
+  if (proj_count <= 0 || iterations < 0 || sirt_count < 1)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_sart_run: invalid counts");
+  for (int i = 0; i < proj_count; ++i)
+    if (index_list[i] < 0 || index_list[i] >= r->cfg.n_proj)
+      return fail(ESB_ERR_INVALID_ARGUMENT, "esb_sart_run: index list entry out of range");
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y;
+  const size_t img = (size_t)W * H;
+  while ((int)r->sirt_d.size() < sirt_count) {
+    float* p = nullptr;
+    ESB_CK(cudaMalloc(&p, img * sizeof(float)), "esb_sart_run");
+    r->sirt_d.push_back(p);
+  }
+  int rc;
+  // EmSart.cpp:579-675
+  for (int iter = 0; iter < iterations; ++iter) {
+    const int steps = (proj_count + sirt_count - 1) / sirt_count;
+    for (int s = 0; s < steps; ++s) {
+      for (int i = 0; i < sirt_count; ++i) {
+        if (s * sirt_count + i >= proj_count) continue;
+        const int index = index_list[s * sirt_count + i];
+        if ((rc = esb_rec_reset_projections(r))) return rc;
+        if ((rc = esb_rec_forward_projection(r, vg, vol, voxel_type, index, *volume_is_empty))) return rc;
+        if ((rc = esb_rec_compare(r, vg, projections + (size_t)index * img, index))) return rc;
+        ESB_CK(cudaMemcpyAsync(r->sirt_d[i], r->proj_d, img * sizeof(float), cudaMemcpyDeviceToDevice, r->stream),
+               "esb_sart_run");
+      }
+      for (int i = 0; i < sirt_count; ++i) {
+        if (s * sirt_count + i >= proj_count) continue;
+        *volume_is_empty = 0;
+        const int index = index_list[s * sirt_count + i];
+        if ((rc = rec_back_project_image(r, vg, vol, voxel_type, index, (float)sirt_count, r->sirt_d[i]))) return rc;
+      }
+    }
+  }
+  return ok();
+}
+
+int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_particles, const esb_vol_geom* sub_geoms,
+                      const esb_proj_geom* pair_geoms, const unsigned char* active, float* const* boxes,
+                      const float* projections, const int* index_list, int proj_count, int batched) {
+  if (!r || !full_vol || !sub_geoms || !pair_geoms || !boxes || !projections || !index_list || n_particles < 0 ||
+      proj_count < 0)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_subvolume_wbp: invalid argument");
+  (void)batched;
+  const esb_recon_config& cf = r->cfg;
+  const int W = cf.proj_x, H = cf.proj_y, np = cf.n_proj;
+  const size_t img = (size_t)W * H;
+  int rc;
+  // EmSartSubVolumes.cpp:626-683 with Reconstructor.cpp:893-914 / 975-1033
+  for (int ii = 0; ii < proj_count; ++ii) {
+    const int index = index_list[ii];
+    if (index < 0 || index >= np) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_subvolume_wbp: index out of range");
+    const float* proj = projections + (size_t)index * img;
+    if (!cf.ctf_mode) {
+      for (int p = 0; p < n_particles; ++p) {
+        if (active && !active[(size_t)p * np + index]) continue;
+        KConst c = rec_const(r, pair_geoms[(size_t)p * np + index], sub_geoms[p], 1);
+        PhaseScope ps(r, 1);
+        ESB_CK(launch_bp(c, boxes[p], ESB_VOXEL_F32, proj, W, H, W, 1.0f, cf.oversampling, 0.0f, 9999999999999.0f, 0,
+                         r->stream), "esb_subvolume_wbp");
+      }
+      continue;
+    }
+    float t_in, t_out;
+    esb_defocus_distances(&r->geoms[index], full_vol, W, H, &t_in, &t_out);
+    const float step = cf.ctf_slice_thickness_nm / cf.pixel_size_nm;
+    for (float ray = t_in; ray < t_out; ray += step) {
+      float dmin, dmax;
+      esb_defocus_min_max(ray, r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index], cf.add_tilt_angle,
+                          cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2], cf.ignore_z_shift_for_ctf,
+                          cf.switch_ctf_direction, &dmin, &dmax);
+      static const int none[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      // makeSquare without crop on the prepared projection (Reconstructor.cpp:995-1004)
+      if ((rc = rec_ctf_chain(r, const_cast<float*>(proj), 0, none, index, dmin, dmax, 0, r->dist_d, nullptr, 0, none))) return rc;
+      for (int p = 0; p < n_particles; ++p) {
+        if (active && !active[(size_t)p * np + index]) continue;
+        KConst c = rec_const(r, pair_geoms[(size_t)p * np + index], sub_geoms[p], 1);
+        PhaseScope ps(r, 1);
+        ESB_CK(launch_bp(c, boxes[p], ESB_VOXEL_F32, r->dist_d, W, H, W, 1.0f, cf.oversampling, ray, ray + step, 1,
+                         r->stream), "esb_subvolume_wbp");
+      }
+    }
+  }
+  return ok();
+}
+
+}  // extern "C"

@@ -1,0 +1,397 @@
+// Image-space kernels of the reconstruction path: residual ("compare"),
+// volume-shadow crop, pad-to-square, the Fourier-space filters (CTF, WBP
+// weighting, band-pass, dose weighting), the fused pre/post-FFT passes of the
+// CTF chain and volume storage conversions.
+#include <math.h>
+
+#include "esb_device.cuh"
+
+namespace esb {
+
+__device__ __forceinline__ float taper(float w) {
+  if (w < 0.0f) w = 0.0f;
+  return 1.0f - expf(-(w * w * 9.0f));
+}
+
+// Kernel `compare` (Compare.cu:50-130). The upper-border factors of the
+// reference evaluate to w = (-y - cut)/dim <= 0, i.e. a hard zero band of
+// width dim+cut; the expressions are kept as written.
+__global__ void k_compare(int pw, int ph, size_t pitchE, const float* __restrict__ real, float* __restrict__ virt,
+                          const float* __restrict__ dist, float realLength, float4 cut, float4 dim, float scale) {
+  const unsigned x = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= (unsigned)pw || y >= (unsigned)ph) return;
+  const size_t i = (size_t)y * pitchE + x;
+  float val = dist[i];
+  float error;
+  if (val >= 1.0f) error = ((real[i]) - ((virt[i] / scale) / val * realLength)) / realLength * scale;
+  else error = 0.0f;
+  float yb = 1.f, ya = 1.f, xb = 1.f, xa = 1.f;
+  const float fy = (float)y, fx = (float)x;
+  if (fy < cut.z + dim.z) yb = taper((fy - cut.z) / dim.z);
+  if (fy > (float)ph - dim.w - cut.w - 1.0f) ya = taper(((float)((unsigned)ph - y - 1u) - cut.w - (float)(ph - 1)) / dim.w);
+  if (fx < cut.y + dim.y) xb = taper((fx - cut.y) / dim.y);
+  if (fx > (float)pw - dim.x - cut.x - 1.0f) xa = taper(((float)((unsigned)pw - x - 1u) - cut.x - (float)(pw - 1)) / dim.x);
+  virt[i] = xa * xb * ya * yb * error;
+}
+
+__device__ __forceinline__ float seg_dist(int2 v, int2 w, int x, int y) {  // Compare.cu:137-163
+  float l2 = (float)((v.x - w.x) * (v.x - w.x) + (v.y - w.y) * (v.y - w.y));
+  auto d = [](float ax, float ay, float bx, float by) { return sqrtf((ax - bx) * (ax - bx) + (ay - by) * (ay - by)); };
+  if (l2 == 0.0f) return d((float)v.x, (float)v.y, (float)x, (float)y);
+  float x1 = (float)(x - v.x), y1 = (float)(y - v.y), x2 = (float)(w.x - v.x), y2 = (float)(w.y - v.y);
+  float t = (x1 * x2 + y1 * y2) / l2;
+  if (t < 0.0f) return d((float)x, (float)y, (float)v.x, (float)v.y);
+  if (t > 1.0f) return d((float)x, (float)y, (float)w.x, (float)w.y);
+  float x3 = v.x + t * (w.x - v.x), y3 = v.y + t * (w.y - v.y);
+  return d((float)x, (float)y, x3, y3);
+}
+
+// Mask factor of kernel `cropBorder` (Compare.cu:171-277) at pixel (x, y).
+__device__ __forceinline__ float crop_factor(int pw, int ph, int x, int y, float2 cut, float2 dim, int2 p1, int2 p2,
+                                             int2 p3, int2 p4) {
+  float dX = 0.f, dY = 0.f;
+  if ((p2.x - p1.x) * (y - p1.y) - (p2.y - p1.y) * (x - p1.x) < 0 &&
+      (p3.x - p4.x) * (y - p4.y) - (p3.y - p4.y) * (x - p4.x) < 0 &&
+      (p1.x - p3.x) * (y - p3.y) - (p1.y - p3.y) * (x - p3.x) < 0 &&
+      (p4.x - p2.x) * (y - p2.y) - (p4.y - p2.y) * (x - p2.x) < 0) {
+    dX = 1.f;
+    dY = 1.f;
+    float mx = 3.0f * pw, my = 3.0f * ph;
+    mx = fminf(mx, seg_dist(p1, p2, x, y));
+    mx = fminf(mx, seg_dist(p4, p3, x, y));
+    mx = fminf(mx, (float)x);
+    mx = fminf(mx, (float)(pw - x - 1));
+    my = fminf(my, seg_dist(p3, p1, x, y));
+    my = fminf(my, seg_dist(p2, p4, x, y));
+    my = fminf(my, (float)y);
+    my = fminf(my, (float)(ph - y - 1));
+    if (mx < cut.x + dim.x) dX = taper((mx - cut.x) / dim.x);
+    if (my < cut.y + dim.y) dY = taper((my - cut.y) / dim.y);
+  }
+  return dX * dY;
+}
+
+__global__ void k_crop_border(int pw, int ph, size_t pitchE, float* __restrict__ img, float2 cut, float2 dim, int2 p1,
+                              int2 p2, int2 p3, int2 p4) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= pw || y >= ph) return;
+  const size_t i = (size_t)y * pitchE + x;
+  img[i] = crop_factor(pw, ph, x, y, cut, dim, p1, p2, p3, p4) * img[i];
+}
+
+// Kernel `makeSquare` (CopyToSquare.cu:38-92).
+__global__ void k_make_square(int pw, int ph, int maxsize, size_t strideE, const float* __restrict__ in,
+                              float* __restrict__ out, int bx, int by, int mirrorY, int fillZero) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= maxsize || y >= maxsize) return;
+  if (fillZero) {
+    float val = 0.f;
+    int xi = x - bx, yi = y - by;
+    if (xi >= 0 && xi < pw && yi >= 0 && yi < ph) {
+      if (mirrorY) yi = ph - yi - 1;
+      val = in[(size_t)yi * strideE + xi];
+    }
+    out[(size_t)y * maxsize + x] = val;
+  } else {
+    int xi = x - bx;
+    if (xi < 0) xi = -xi - 1;
+    if (xi >= pw) { xi = xi - pw; xi = pw - xi - 1; }
+    int yi = y - by;
+    if (yi < 0) yi = -yi - 1;
+    if (yi >= ph) { yi = yi - ph; yi = ph - yi - 1; }
+    if (mirrorY) yi = ph - yi - 1;
+    out[(size_t)y * maxsize + x] = in[(size_t)yi * strideE + xi];
+  }
+}
+
+// Fused cropBorder (in place on img, the reference applies it to proj_d /
+// dist_d before padding) + makeSquare with zero fill (Reconstructor.cpp:566-568,
+// 954-956).
+__global__ void k_crop_to_square(int pw, int ph, size_t pitchE, float* __restrict__ img, int apply_crop, float2 cut,
+                                 float2 dim, int2 p1, int2 p2, int2 p3, int2 p4, int maxsize, float* __restrict__ sq,
+                                 int bx, int by) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= maxsize || y >= maxsize) return;
+  int xi = x - bx, yi = y - by;
+  float val = 0.f;
+  if (xi >= 0 && xi < pw && yi >= 0 && yi < ph) {
+    const size_t i = (size_t)yi * pitchE + xi;
+    val = img[i];
+    if (apply_crop) {
+      val = crop_factor(pw, ph, xi, yi, cut, dim, p1, p2, p3, p4) * val;
+      img[i] = val;
+    }
+  }
+  sq[(size_t)y * maxsize + x] = val;
+}
+
+// Fused nppiDivC (by N*N, centred W x H window) + cropBorder + optional
+// accumulation into proj (Reconstructor.cpp:578-583, 962-965).
+__global__ void k_square_to_image(const float* __restrict__ sq, int maxsize, size_t shift, float inv_norm, int pw,
+                                  int ph, size_t pitchE, float* __restrict__ out, float* __restrict__ accum,
+                                  int apply_crop, float2 cut, float2 dim, int2 p1, int2 p2, int2 p3, int2 p4) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= pw || y >= ph) return;
+  float v = sq[shift + (size_t)y * maxsize + x] * inv_norm;
+  if (apply_crop) v = crop_factor(pw, ph, x, y, cut, dim, p1, p2, p3, p4) * v;
+  const size_t i = (size_t)y * pitchE + x;
+  if (out) out[i] = v;
+  if (accum) accum[i] += v;
+}
+
+// Kernel `ctf` (ctf.cu:82-240).
+__global__ void k_ctf(float2* __restrict__ spec, int n, CtfConst k, float d0, float d1, float angle, int applyForFP,
+                      int phaseFlipOnly, float wiener, float4 beta) {
+  const unsigned x = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= (unsigned)(n / 2 + 1) || y >= (unsigned)n) return;
+  const float PI = 3.14159265358979323846f;
+  float xpos = (float)x, ypos = (float)y;
+  if (ypos > k.pixelcount * 0.5f) ypos = (k.pixelcount - ypos) * -1.0f;
+  float alpha = (xpos == 0.f) ? (PI * 0.5f) : atan2f(ypos, xpos);
+  float beta_ = alpha - angle;
+  float defocus = d0 + (1.f - cosf(2.f * beta_)) * (d1 - d0);
+  float radius = sqrtf(xpos * xpos + ypos * ypos);
+  float length = radius * k.freqStep;
+  float L = k.lambda;
+  float m = (PI / 2.0f) * (k.cs * L * L * L * length * length * length * length - 2.f * defocus * L * length * length);
+  float nn = k.phaseC * sinf(m) + k.ampC * cosf(m);
+  const size_t i = (size_t)y * (n / 2 + 1) + x;
+  float2 res = spec[i];
+  if (applyForFP && radius > beta.x && !phaseFlipOnly) {
+    float l = length / 100000000.0f;
+    float e = expf(-beta.y * l - beta.z * l * l - beta.w * l * l * l);
+    e = fmaxf(e, 0.01f);
+    float val = nn * e;
+    if (fabsf(val) < 0.0001f && val >= 0.f) val = 0.0001f;
+    if (fabsf(val) < 0.0001f && val < 0.f) val = -0.0001f;
+    res.x = res.x * -val;
+    res.y = res.y * -val;
+  }
+  if (!applyForFP && radius > beta.x && !phaseFlipOnly) {
+    float l = length / 100000000.0f;
+    float e = expf(-beta.y * l - beta.z * l * l - beta.w * l * l * l);
+    e = fmaxf(e, wiener);
+    float val = nn * e;
+    float f = -val / (val * val + wiener);
+    res.x = res.x * f;
+    res.y = res.y * f;
+  }
+  if (phaseFlipOnly && nn >= 0.f) {
+    res.x = -res.x;
+    res.y = -res.y;
+  }
+  spec[i] = res;
+}
+
+// Kernel `wbpWeighting` (wbpWeighting.cu:50-144).
+__global__ void k_wbp_weighting(float2* __restrict__ spec, int n, float s, float co, int fm) {
+  const unsigned x = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= (unsigned)(n / 2 + 1) || y >= (unsigned)n) return;
+  float xp = (float)x, yp = (float)y;
+  if (yp > n * 0.5f) yp = (n - yp) * -1.0f;
+  float yr = s * xp + co * yp;
+  float length = yr / n / 2.0f;
+  float w = 1.0f;
+  if (fm == 0) {
+    w = fminf(fabsf(length), 1.0f);
+  } else if (fm >= 2 && fm <= 4) {
+    const float P[3][4] = {{1.000654227857550f, 0.006008581017124f, 0.004159659493151f, 0.000975903396538f},
+                           {1.003784816598589f, 0.029016377161629f, 0.019582940715148f, 0.004559409669984f},
+                           {0.999884616010943f, 0.000307646262566f, 0.004742915272196f, 0.004806551368900f}};
+    const float* p = P[fm - 2];
+    if (length == 0.f) w = 0.f;
+    else {
+      float lf = logf(fabsf(length));
+      w = p[0] + p[1] * lf + p[2] * lf * lf + p[3] * lf * lf * lf;
+    }
+    w = fmaxf(0.f, fminf(w, 1.f));
+  }
+  const size_t i = (size_t)y * (n / 2 + 1) + x;
+  float2 r = spec[i];
+  r.x *= w;
+  r.y *= w;
+  spec[i] = r;
+}
+
+// Kernel `fourierFilter` (wbpWeighting.cu:148-212).
+__global__ void k_fourier_filter(float2* __restrict__ spec, int n, float lp, float hp, float lps, float hps) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= n / 2 + 1 || y >= n) return;
+  float mx = (float)x, my = (float)y;
+  if (my > n * 0.5f) my = (n - my) * -1.0f;
+  float dist = sqrtf(mx * mx + my * my);
+  float fil = 0.f;
+  lp = lp - lps;
+  hp = hp + hps;
+  if (lp > 0) { if (dist <= lp) fil = 1.f; }
+  else { if (dist <= n / 2 - 1) fil = 1.f; }
+  if (lps > 0) {
+    float fil2 = (-fil + 1.0f) * expf(-((dist - lp) * (dist - lp) / (2 * lps * lps)));
+    if (fil2 > 0.001f) fil = fil2;
+  }
+  if (lps > 0 && lp == 0 && hp == 0 && hps == 0) fil = expf(-((dist - lp) * (dist - lp) / (2 * lps * lps)));
+  if (hp > 0) {
+    float fil2 = 0.f;
+    if (dist >= hp) fil2 = 1.f;
+    fil *= fil2;
+    if (hps > 0) {
+      float fil3 = (-fil2 + 1) * expf(-((dist - hp) * (dist - hp) / (2 * hps * hps)));
+      if (fil3 > 0.001f) fil = fil3;
+    }
+  }
+  const size_t i = (size_t)y * (n / 2 + 1) + x;
+  float2 r = spec[i];
+  r.x *= fil;
+  r.y *= fil;
+  spec[i] = r;
+}
+
+// Kernel `doseWeighting` (wbpWeighting.cu:216-240).
+__global__ void k_dose_weighting(float2* __restrict__ spec, int n, float dose, float pixelsize) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= n / 2 + 1 || y >= n) return;
+  float mx = (float)x, my = (float)y;
+  if (my > n * 0.5f) my = (n - my) * -1.0f;
+  float dist = sqrtf(mx * mx + my * my);
+  dist = dist / (float)(n / 2 / pixelsize);
+  float fil = expf(-dose * dist);
+  const size_t i = (size_t)y * (n / 2 + 1) + x;
+  float2 r = spec[i];
+  r.x *= fil;
+  r.y *= fil;
+  spec[i] = r;
+}
+
+template <int VT>
+__global__ void k_convert(const void* __restrict__ vol, long n, float* __restrict__ out, float sign) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = sign * Voxel<VT>::loadrw(vol, i);
+}
+template <int VT>
+__global__ void k_store(const float* __restrict__ in, long n, void* __restrict__ vol) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    Voxel<VT>::store(vol, i, in[i]);
+}
+
+// ----------------------------------------------------------------- launchers
+static inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
+
+cudaError_t launch_compare(int pw, int ph, size_t pitchE, const float* real, float* virt, const float* dist,
+                           float realLength, float4 cut, float4 dim, float scale, cudaStream_t st) {
+  dim3 b(32, 8);
+  k_compare<<<grid2(pw, ph, b), b, 0, st>>>(pw, ph, pitchE, real, virt, dist, realLength, cut, dim, scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crop_border(int pw, int ph, size_t pitchE, float* img, float2 cut, float2 dim, const int* p,
+                               cudaStream_t st) {
+  dim3 b(32, 8);
+  k_crop_border<<<grid2(pw, ph, b), b, 0, st>>>(pw, ph, pitchE, img, cut, dim, make_int2(p[0], p[1]),
+                                                 make_int2(p[2], p[3]), make_int2(p[4], p[5]), make_int2(p[6], p[7]));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_make_square(int pw, int ph, size_t strideE, const float* in, int maxsize, float* out, int bx,
+                               int by, int mirrorY, int fillZero, cudaStream_t st) {
+  dim3 b(32, 8);
+  k_make_square<<<grid2(maxsize, maxsize, b), b, 0, st>>>(pw, ph, maxsize, strideE, in, out, bx, by, mirrorY, fillZero);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crop_to_square(int pw, int ph, size_t pitchE, float* img, int apply_crop, float2 cut, float2 dim,
+                                  const int* p, int maxsize, float* sq, int bx, int by, cudaStream_t st) {
+  dim3 b(32, 8);
+  k_crop_to_square<<<grid2(maxsize, maxsize, b), b, 0, st>>>(pw, ph, pitchE, img, apply_crop, cut, dim,
+                                                            make_int2(p[0], p[1]), make_int2(p[2], p[3]),
+                                                            make_int2(p[4], p[5]), make_int2(p[6], p[7]), maxsize, sq,
+                                                            bx, by);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_square_to_image(const float* sq, int maxsize, size_t shift, float inv_norm, int pw, int ph,
+                                   size_t pitchE, float* out, float* accum, int apply_crop, float2 cut, float2 dim,
+                                   const int* p, cudaStream_t st) {
+  dim3 b(32, 8);
+  k_square_to_image<<<grid2(pw, ph, b), b, 0, st>>>(sq, maxsize, shift, inv_norm, pw, ph, pitchE, out, accum,
+                                                    apply_crop, cut, dim, make_int2(p[0], p[1]), make_int2(p[2], p[3]),
+                                                    make_int2(p[4], p[5]), make_int2(p[6], p[7]));
+  return cudaGetLastError();
+}
+
+CtfConst make_ctf_const(int n, float cs_mm, float voltage_kv, float amp_contrast, float pixel_size_nm) {
+  // SetConstantValues(CTFKernel, ...) (Kernels.cpp:1104-1131) and the
+  // wavelength macro of ctf.cu:62.
+  CtfConst k;
+  float pixelsize = pixel_size_nm * powf(10.0f, -9.0f);
+  k.pixelcount = (float)n;
+  float maxFreq = (float)(1.0 / (pixelsize * 2.0f));
+  k.freqStep = maxFreq / (k.pixelcount / 2.0f);
+  k.ampC = amp_contrast;
+  k.phaseC = sqrtf(1.0f - amp_contrast * amp_contrast);
+  float hc = ((float)6.63E-34) * ((float)3.00E+08);
+  double X = (double)(2 * 511 * voltage_kv * 1000.0f * 1000.0f) + (double)(voltage_kv * voltage_kv * 1000.0f * 1000.0f);
+  k.lambda = hc / (float)sqrt((float)(X * 1.602E-19 * 1.602E-19));
+  k.cs = cs_mm * 0.001f;
+  return k;
+}
+
+cudaError_t launch_ctf(float* spec, int n, const CtfConst& k, float d0_nm, float d1_nm, float angle_deg,
+                       int applyForFP, int phaseFlip, float wiener, float4 beta, cudaStream_t st) {
+  dim3 b(32, 8);
+  float d0 = d0_nm * 0.000000001f, d1 = d1_nm * 0.000000001f;
+  float ang = angle_deg / 180.0f * 3.14159265358979323846f;
+  k_ctf<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, k, d0, d1, ang, applyForFP, phaseFlip, wiener, beta);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wbp_weighting(float* spec, int n, float psi_deg, int fm, cudaStream_t st) {
+  dim3 b(32, 8);
+  float a = -psi_deg / 180.0f * 3.14159265358979323846f;
+  k_wbp_weighting<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, (float)sin((double)a), (float)cos((double)a), fm);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fourier_filter(float* spec, int n, float lp, float hp, float lps, float hps, cudaStream_t st) {
+  dim3 b(32, 8);
+  k_fourier_filter<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, lp, hp, lps, hps);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dose_weighting(float* spec, int n, float dose, float pixelsize, cudaStream_t st) {
+  dim3 b(32, 8);
+  k_dose_weighting<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, dose, pixelsize);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert(const void* vol, int vt, long n, float* out, float sign, cudaStream_t st) {
+  int blocks = (int)((n + 255) / 256 < 148 * 32 ? (n + 255) / 256 : 148 * 32);
+  if (blocks < 1) blocks = 1;
+  switch (vt) {
+    case ESB_VOXEL_F32: k_convert<ESB_VOXEL_F32><<<blocks, 256, 0, st>>>(vol, n, out, sign); break;
+    case ESB_VOXEL_F16: k_convert<ESB_VOXEL_F16><<<blocks, 256, 0, st>>>(vol, n, out, sign); break;
+    default: k_convert<ESB_VOXEL_BF16><<<blocks, 256, 0, st>>>(vol, n, out, sign); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_store(const float* in, long n, void* vol, int vt, cudaStream_t st) {
+  int blocks = (int)((n + 255) / 256 < 148 * 32 ? (n + 255) / 256 : 148 * 32);
+  if (blocks < 1) blocks = 1;
+  switch (vt) {
+    case ESB_VOXEL_F32: k_store<ESB_VOXEL_F32><<<blocks, 256, 0, st>>>(in, n, vol); break;
+    case ESB_VOXEL_F16: k_store<ESB_VOXEL_F16><<<blocks, 256, 0, st>>>(in, n, vol); break;
+    default: k_store<ESB_VOXEL_BF16><<<blocks, 256, 0, st>>>(in, n, vol); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace esb

@@ -1,0 +1,380 @@
+"""Python host layer over libesb: the EmSART reconstruction calls.
+
+Mirrors the reference's host interface for the hot path:
+
+* geometry: ``Projection`` (src/EmSART/Projection.h:50-87) and ``Volume``
+  (src/EmSART/Volume.h:30-79). Both are computed in C++ by libesb.
+* kernel wrappers: FPKernel, SlicerKernel, VolTravLengthKernel, CompKernel,
+  CropBorderKernel, BPKernel, CTFKernel, CopyToSquareKernel,
+  WbpWeightingKernel, FourFilterKernel, DoseWeightingKernel
+  (src/EmSART/Kernels.h:37-245).
+* ``Reconstructor`` (src/EmSART/Reconstructor.h:181-249), the SART driver
+  loop of EmSart.cpp:579-675, and the sub-volume back-projection of
+  EmSartSubVolumes.cpp:611-705.
+
+Device buffers are torch CUDA tensors, used only as memory. Every
+computation runs in libesb's CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check, fptr, lib
+
+VOXEL_F32, VOXEL_F16, VOXEL_BF16 = L.VOXEL_F32, L.VOXEL_F16, L.VOXEL_BF16
+PLT_NORMAL, PLT_RANDOM, PLT_RANDOM_START_ZERO_TILT = 0, 1, 2
+FM_RAMP, FM_EXACT, FM_CONTRAST2, FM_CONTRAST10, FM_CONTRAST30 = range(5)
+
+_TORCH_DTYPES = None
+
+
+def _voxel_type_of(t) -> int:
+    import torch
+
+    return {torch.float32: VOXEL_F32, torch.float16: VOXEL_F16, torch.bfloat16: VOXEL_BF16}[t.dtype]
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def _f32(a, n=None) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+# --------------------------------------------------------------------------- geometry
+@dataclass
+class Markers:
+    """Per-projection alignment items of the marker file (MarkerFile.h:34-46)."""
+
+    tilt_angle: np.ndarray
+    x_shift: Optional[np.ndarray] = None
+    y_shift: Optional[np.ndarray] = None
+    magnification: Optional[np.ndarray] = None
+    rotation_psi: Optional[np.ndarray] = None
+
+    @property
+    def count(self) -> int:
+        return int(np.asarray(self.tilt_angle).size)
+
+
+@dataclass
+class TiltConfig:
+    add_tilt_angle: float = 0.0
+    add_tilt_x_angle: float = 0.0
+    use_fix_psi_angle: bool = False
+    psi_angle: float = 0.0
+    phi_angle: float = 0.0
+
+    def c(self) -> L.TiltConfig:
+        return L.TiltConfig(self.add_tilt_angle, self.add_tilt_x_angle, int(self.use_fix_psi_angle),
+                            self.psi_angle, self.phi_angle)
+
+
+def projection_geometry(markers: Markers, width: int, height: int, cfg: TiltConfig = TiltConfig(),
+                        extra_shift=None):
+    """Detector frames of all projections: a ctypes array of ProjGeom."""
+    n = markers.count
+    out = (L.ProjGeom * n)()
+    arrs = [_f32(markers.tilt_angle, n)]
+    for a in (markers.x_shift, markers.y_shift, markers.magnification, markers.rotation_psi):
+        arrs.append(None if a is None else _f32(a, n))
+    es = None if extra_shift is None else _f32(extra_shift, 2 * n)
+    check(lib.esb_projection_geometry(n, width, height, *[fptr(a) for a in arrs], fptr(es), C.byref(cfg.c()),
+                                      C.cast(out, C.c_void_p)))
+    return out
+
+
+def volume_geometry(dims: Sequence[int], voxel_size=(1.0, 1.0, 1.0), volume_shift=(0.0, 0.0, 0.0),
+                    subvol_count: int = 1, subvol: int = 0) -> L.VolGeom:
+    """Volume(dims, count, part) + PositionInSpace (Volume.cpp:82-114, 270-287)."""
+    d = np.asarray(dims, dtype=np.int32)
+    vs = _f32(voxel_size if np.size(voxel_size) == 3 else [voxel_size] * 3, 3)
+    sh = _f32(volume_shift, 3)
+    g = L.VolGeom()
+    check(lib.esb_volume_geometry(fptr(d), subvol_count, subvol, fptr(vs), fptr(sh), C.byref(g)))
+    return g
+
+
+def subvolume_geometry(size: int, voxel_size_sub: float, vol: L.VolGeom, pos, shift=(0, 0, 0)) -> L.VolGeom:
+    g = L.VolGeom()
+    check(lib.esb_subvolume_geometry(size, voxel_size_sub, C.byref(vol), fptr(_f32(pos, 3)), fptr(_f32(shift, 3)),
+                                     C.byref(g)))
+    return g
+
+
+def mag_aniso_matrix(amount: float, angle_deg: float, dim_x: float, dim_y: float) -> np.ndarray:
+    out = np.zeros(9, np.float32)
+    check(lib.esb_mag_aniso_matrix(amount, angle_deg, dim_x, dim_y, fptr(out)))
+    return out
+
+
+IDENTITY3 = np.eye(3, dtype=np.float32).ravel()
+
+
+def set_constant_values(pg: L.ProjGeom, vg: L.VolGeom, mag=None, mag_inv=None, for_bp: bool = False) -> L.Constants:
+    c = L.Constants()
+    m = _f32(IDENTITY3 if mag is None else mag, 9)
+    mi = _f32(IDENTITY3 if mag_inv is None else mag_inv, 9)
+    check(lib.esb_set_constant_values(C.byref(pg), C.byref(vg), fptr(m), fptr(mi), int(for_bp), C.byref(c)))
+    return c
+
+
+def compute_hit_points(pg: L.ProjGeom, vg: L.VolGeom) -> np.ndarray:
+    out = np.zeros(8, np.int32)
+    check(lib.esb_compute_hit_points(C.byref(pg), C.byref(vg), fptr(out)))
+    return out
+
+
+def defocus_distances(pg: L.ProjGeom, vg: L.VolGeom, width: int, height: int):
+    a, b = C.c_float(), C.c_float()
+    check(lib.esb_defocus_distances(C.byref(pg), C.byref(vg), width, height, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def projection_index_list(kind: int, tilt_deg, good=None) -> np.ndarray:
+    t = _f32(tilt_deg)
+    n = t.size
+    g = None if good is None else np.ascontiguousarray(np.asarray(good, np.int32))
+    out = np.zeros(n, np.int32)
+    cnt = C.c_int()
+    check(lib.esb_projection_index_list(kind, n, fptr(t), fptr(g), fptr(out), C.byref(cnt)))
+    return out[: cnt.value].copy()
+
+
+# --------------------------------------------------------------------------- kernels
+def _img_args(img):
+    h, w = img.shape[-2:]
+    return w, h, img.stride(-2) * 4
+
+
+def forward_project(c: L.Constants, vol, proj, dist, roi=None, stream=None) -> None:
+    """FPKernel: proj += line integrals, dist = mean chord (Kernels.cpp:46-88)."""
+    w, h, pitch = _img_args(proj)
+    x0, y0, x1, y1 = roi if roi is not None else (0, 0, w, h)
+    check(lib.esb_fp(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(proj), fptr(dist), pitch, x0, y0, x1, y1,
+                     _stream(stream)))
+
+
+def forward_project_slab(c: L.Constants, vol, proj, tmin: float, tmax: float, roi=None, stream=None) -> None:
+    w, h, pitch = _img_args(proj)
+    x0, y0, x1, y1 = roi if roi is not None else (0, 0, w, h)
+    check(lib.esb_fp_slicer(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(proj), pitch, tmin, tmax, x0, y0,
+                            x1, y1, _stream(stream)))
+
+
+def traversal_length(c: L.Constants, dist, roi=None, stream=None) -> None:
+    w, h, pitch = _img_args(dist)
+    x0, y0, x1, y1 = roi if roi is not None else (0, 0, w, h)
+    check(lib.esb_vol_traversal_length(C.byref(c), w, h, fptr(dist), pitch, x0, y0, x1, y1, _stream(stream)))
+
+
+def compare(real, virt, dist, real_length: float, crop=(0, 0, 0, 0), crop_dim=(0, 0, 0, 0), scale: float = 1.0,
+            stream=None) -> None:
+    w, h, pitch = _img_args(virt)
+    check(lib.esb_compare(w, h, pitch, fptr(real), fptr(virt), fptr(dist), real_length, fptr(_f32(crop, 4)),
+                          fptr(_f32(crop_dim, 4)), scale, _stream(stream)))
+
+
+def crop_border(img, cut_length, dim_length, points, stream=None) -> None:
+    w, h, pitch = _img_args(img)
+    p = np.ascontiguousarray(np.asarray(points, np.int32).ravel())
+    check(lib.esb_crop_border(w, h, pitch, fptr(img), fptr(_f32(cut_length, 2)), fptr(_f32(dim_length, 2)), fptr(p),
+                              _stream(stream)))
+
+
+def back_project(c: L.Constants, vol, img, lam: float, oversampling: int = 1, dist_min: float = 0.0,
+                 dist_max: float = 9999999999999.0, linear: bool = False, stream=None) -> None:
+    """BPKernel: vol += lam * sum(img*chord)/sum(chord) (Kernels.cpp:327-379)."""
+    w, h, pitch = _img_args(img)
+    check(lib.esb_bp(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(img), pitch, lam, oversampling, dist_min,
+                     dist_max, int(linear), _stream(stream)))
+
+
+def make_square(img, maxsize: int, out, border_x: int, border_y: int, mirror_y=False, fill_zero=True, stream=None):
+    w, h, pitch = _img_args(img)
+    check(lib.esb_make_square(w, h, pitch, fptr(img), maxsize, fptr(out), border_x, border_y, int(mirror_y),
+                              int(fill_zero), _stream(stream)))
+
+
+def ctf(spectrum, n: int, defocus_min_nm: float, defocus_max_nm: float, angle_deg: float, apply_for_fp: bool,
+        phase_flip_only: bool = False, wiener: float = 0.1, beta_fac=(200, 0, 0.008, 0), cs_mm: float = 2.7,
+        voltage_kv: float = 300.0, amp_contrast: float = 0.0, pixel_size_nm: float = 0.27, stream=None) -> None:
+    check(lib.esb_ctf(fptr(spectrum), n, defocus_min_nm, defocus_max_nm, angle_deg, int(apply_for_fp),
+                      int(phase_flip_only), wiener, fptr(_f32(beta_fac, 4)), cs_mm, voltage_kv, amp_contrast,
+                      pixel_size_nm, _stream(stream)))
+
+
+def wbp_weighting(spectrum, n: int, psi_deg: float, method: int = FM_RAMP, stream=None) -> None:
+    check(lib.esb_wbp_weighting(fptr(spectrum), n, psi_deg, method, _stream(stream)))
+
+
+def fourier_filter(spectrum, n: int, lp: float, hp: float, lps: float, hps: float, stream=None) -> None:
+    check(lib.esb_fourier_filter(fptr(spectrum), n, lp, hp, lps, hps, _stream(stream)))
+
+
+def dose_weighting(spectrum, n: int, dose: float, pixel_size_a: float, stream=None) -> None:
+    check(lib.esb_dose_weighting(fptr(spectrum), n, dose, pixel_size_a, _stream(stream)))
+
+
+def convert_volume(vol, out, negate: bool = False, stream=None) -> None:
+    check(lib.esb_convert_volume(fptr(vol), _voxel_type_of(vol), vol.numel(), fptr(out), int(negate), _stream(stream)))
+
+
+def store_volume(src, vol, stream=None) -> None:
+    check(lib.esb_store_volume(fptr(src), src.numel(), fptr(vol), _voxel_type_of(vol), _stream(stream)))
+
+
+class _CudaArray:
+    def __init__(self, address: int, shape, typestr: str = "<f4"):
+        self.__cuda_array_interface__ = {"data": (int(address), False), "shape": tuple(shape), "typestr": typestr,
+                                         "version": 2}
+
+
+def device_view(address: int, shape, typestr: str = "<f4"):
+    """Zero-copy torch view of a device buffer owned by libesb."""
+    import torch
+
+    return torch.as_tensor(_CudaArray(address, shape, typestr), device="cuda")
+
+
+# --------------------------------------------------------------------------- reconstructor
+@dataclass
+class ReconConfig:
+    """The emsart.cfg keys the hot path reads (utils/Config.cpp:303-494)."""
+
+    proj_x: int
+    proj_y: int
+    n_proj: int
+    lambda_: float = 1.0
+    oversampling: int = 1
+    ctf_mode: bool = False
+    cut_length: tuple = (0.0, 0.0)
+    dim_length: tuple = (1.0, 1.0)
+    crop: tuple = (0.0, 0.0, 0.0, 0.0)
+    crop_dim: tuple = (1.0, 1.0, 1.0, 1.0)
+    projection_scale_factor: float = 1.0
+    pixel_size_nm: float = 1.0
+    cs_mm: float = 2.7
+    voltage_kv: float = 300.0
+    amp_contrast: float = 0.0
+    ctf_slice_thickness_nm: float = 50.0
+    ctf_beta_fac: tuple = (200.0, 0.0, 0.008, 0.0)
+    wiener_noise_level: float = 0.1
+    phase_flip_only: bool = False
+    ignore_z_shift_for_ctf: bool = False
+    switch_ctf_direction: bool = False
+    volume_shift: tuple = (0.0, 0.0, 0.0)
+    add_tilt_angle: float = 0.0
+
+    def c(self) -> L.ReconConfig:
+        r = L.ReconConfig()
+        r.proj_x, r.proj_y, r.n_proj = self.proj_x, self.proj_y, self.n_proj
+        r.lambda_, r.oversampling, r.ctf_mode = self.lambda_, self.oversampling, int(self.ctf_mode)
+        r.cut_length[:] = list(self.cut_length)
+        r.dim_length[:] = list(self.dim_length)
+        r.crop[:] = list(self.crop)
+        r.crop_dim[:] = list(self.crop_dim)
+        r.projection_scale_factor = self.projection_scale_factor
+        r.pixel_size_nm, r.cs_mm, r.voltage_kv = self.pixel_size_nm, self.cs_mm, self.voltage_kv
+        r.amp_contrast, r.ctf_slice_thickness_nm = self.amp_contrast, self.ctf_slice_thickness_nm
+        r.ctf_beta_fac[:] = list(self.ctf_beta_fac)
+        r.wiener_noise_level, r.phase_flip_only = self.wiener_noise_level, int(self.phase_flip_only)
+        r.ignore_z_shift_for_ctf = int(self.ignore_z_shift_for_ctf)
+        r.switch_ctf_direction = int(self.switch_ctf_direction)
+        r.volume_shift[:] = list(self.volume_shift)
+        r.add_tilt_angle = self.add_tilt_angle
+        return r
+
+
+class Reconstructor:
+    """Owner of the projection buffers, FFT plans and geometry of one GPU
+    (Reconstructor.cpp:203-372)."""
+
+    def __init__(self, cfg: ReconConfig, geoms, tilt_deg, defocus=None, mag=None, mag_inv=None, stream=None):
+        self.cfg = cfg
+        self._geoms = geoms
+        self._tilt = _f32(tilt_deg, cfg.n_proj)
+        self._defocus = None if defocus is None else _f32(defocus, 3 * cfg.n_proj)
+        self._mag = _f32(IDENTITY3 if mag is None else mag, 9)
+        self._mag_inv = _f32(IDENTITY3 if mag_inv is None else mag_inv, 9)
+        h = C.c_void_p()
+        check(lib.esb_reconstructor_create(C.byref(cfg.c()), C.cast(geoms, C.c_void_p), fptr(self._tilt),
+                                           fptr(self._defocus), fptr(self._mag), fptr(self._mag_inv), C.byref(h)))
+        self._h = h
+        check(lib.esb_reconstructor_set_stream(self._h, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.esb_reconstructor_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def buffers(self):
+        """(proj_d, dist_d, real_d) device addresses."""
+        a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib.esb_reconstructor_buffers(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def views(self):
+        """(proj_d, dist_d, real_d) as zero-copy torch views (H x W float32)."""
+        return tuple(device_view(p, (self.cfg.proj_y, self.cfg.proj_x)) for p in self.buffers())
+
+    def reset_projections(self):
+        check(lib.esb_rec_reset_projections(self._h))
+
+    def enable_timing(self, on: bool = True):
+        check(lib.esb_reconstructor_enable_timing(self._h, int(on)))
+
+    def timing(self):
+        """{phase: (ms, launches)} since the previous call; phases fp, bp, ctf, compare."""
+        ms = np.zeros(4, np.float64)
+        cnt = np.zeros(4, np.int32)
+        check(lib.esb_reconstructor_timing(self._h, fptr(ms), fptr(cnt)))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("fp", "bp", "ctf", "compare"))}
+
+    def forward_projection(self, vg, vol, index: int, volume_is_empty: bool = False):
+        check(lib.esb_rec_forward_projection(self._h, C.byref(vg), fptr(vol), _voxel_type_of(vol), index,
+                                             int(volume_is_empty)))
+
+    def compare(self, vg, real, index: int):
+        check(lib.esb_rec_compare(self._h, C.byref(vg), fptr(real), index))
+
+    def back_projection(self, vg, vol, index: int, sirt_count: float = 1.0):
+        check(lib.esb_rec_back_projection(self._h, C.byref(vg), fptr(vol), _voxel_type_of(vol), index, sirt_count))
+
+    def sart(self, vg, vol, projections, index_list, iterations: int, sirt_count: int, volume_is_empty: bool = True):
+        """EmSart.cpp:579-675. Returns the updated volume_is_empty flag."""
+        il = np.ascontiguousarray(np.asarray(index_list, np.int32))
+        empty = C.c_int(int(volume_is_empty))
+        check(lib.esb_sart_run(self._h, C.byref(vg), fptr(vol), _voxel_type_of(vol), fptr(projections), fptr(il),
+                               il.size, iterations, sirt_count, C.byref(empty)))
+        return bool(empty.value)
+
+    def subvolume_wbp(self, full_vg, sub_geoms, pair_geoms, boxes, projections, index_list, active=None,
+                      batched: bool = True):
+        n = len(boxes)
+        sg = (L.VolGeom * n)(*sub_geoms)
+        ptrs = (C.c_void_p * n)(*[b.data_ptr() for b in boxes])
+        act = None if active is None else np.ascontiguousarray(np.asarray(active, np.uint8))
+        il = np.ascontiguousarray(np.asarray(index_list, np.int32))
+        check(lib.esb_subvolume_wbp(self._h, C.byref(full_vg), n, C.cast(sg, C.c_void_p),
+                                    C.cast(pair_geoms, C.c_void_p), fptr(act), C.cast(ptrs, C.c_void_p),
+                                    fptr(projections), fptr(il), il.size, int(batched)))

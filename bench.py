@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the EmSART SART + 3D-CTF iteration on B200.
+
+One step = one SART iteration of the 1024x1024x256 / 61 x 1024^2 / CTF /
+oversampling 2 / 4-projection ordered subsets workload: for every projection
+forward projection over the 30 nm defocus slabs (slicer + CTF chain),
+compare, and per ordered subset the CTF-slab back-projections. The metric is
+voxel-updates per second (one voxel back-projected from one projection,
+forward projection and compare of that projection included).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl esb|reference]
+
+Multi-GPU (torchrun): every rank reconstructs its own tomogram (independent
+tilt series), so the per-GPU work is fixed and scaling is weak; no collective
+runs on the data path. The timing is taken with CUDA events on the
+reconstructor's stream between barriers, maximum over ranks.
+
+--impl reference times the CPU oracle (the multithreaded C++ restatement of
+the reference's kernels; the reference's own GPU code cannot be compiled with
+CUDA 12.9) on a bounded sample of the same workload and prints the same line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SART voxel-updates/s (SART+3D-CTF iteration, 1024x1024x256, 61x1024^2)"
+UNIT = "voxel-updates/s"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_sample(workload_params, n_proj_sample: int = 4, y_extent: int = 8):
+    """Time the CPU oracle on a bounded sample of the workload.
+
+    The sample keeps the full workload's geometry, tilt angles, CTF slabs and
+    1024^2 FFTs but cuts the volume to `y_extent` voxels along the tilt axis
+    (y; the detector's u axis), where the rays of a single-axis tilt series
+    stay in constant-y planes, so the per-voxel and per-pixel work of the
+    projector and back-projector equals the full problem's. The voxel work is
+    extrapolated by the volume ratio; the CTF chain (crop, pad, 1024^2 FFT
+    pair, filter) is counted at full size. Returns (voxel-updates/s, detail).
+    """
+    from oracle import geometry as G
+    from oracle.driver import OracleReconstructor
+    from oracle import driver as D
+    from artiatomi_b200 import phantom as PH
+
+    p = workload_params
+    nx, ny, nz = p["dims"]
+    W, H = p["W"], p["H"]
+    n = p["n_proj"]
+    tilt = PH.tilt_series(n, -60.0, 60.0)
+    xs, ys, psi = PH.alignment(n, seed=0, shift=p.get("shift", 0.0), psi_jitter=0.0)
+    sub_dims = (nx, y_extent, nz)
+    Ws = y_extent  # detector u follows volume y
+    og = G.projection_geometry(tilt, xs, ys, None, psi, Ws, H)
+    vo = G.volume_geometry(sub_dims)
+    vol = PH.phantom_numpy(sub_dims, max(4, p["n_ell"] * y_extent // ny), seed=1)
+    rng = np.random.default_rng(3)
+    defocus = None
+    cfgd = dict(lambda_=p["lam"], oversampling=p["os"], cut_length=(10.0, 10.0), dim_length=(20.0, 20.0))
+    if p["ctf"]:
+        dmid = rng.uniform(2500.0, 3500.0, n)
+        defocus = np.stack([dmid - 50.0, dmid + 50.0, rng.uniform(0.0, 180.0, n)], 1).astype(np.float32).ravel()
+        cfgd.update(ctf_mode=True, pixel_size_nm=0.27, ctf_slice_thickness_nm=30.0)
+    orc = OracleReconstructor(cfgd, Ws, H, og, tilt, defocus, precision=0)
+    orc.N = max(W, H)  # full-size FFTs as in the full workload
+    orc.bx, orc.by = (orc.N - Ws) // 2, (orc.N - H) // 2
+    projs = rng.normal(size=(n, H, Ws)).astype(np.float32)
+    idx = [int(i) for i in np.linspace(0, n - 1, n_proj_sample).round()]
+    t_fp = t_bp = t_ctf = 0.0
+    # time the kernels and the CTF chain separately by wrapping the oracle's steps
+    orig_chain = orc._ctf_chain
+    ctf_time = [0.0]
+
+    def timed_chain(*a, **k):
+        t0 = time.perf_counter()
+        r = orig_chain(*a, **k)
+        ctf_time[0] += time.perf_counter() - t0
+        return r
+
+    orc._ctf_chain = timed_chain
+    t0 = time.perf_counter()
+    for i in idx:
+        orc.reset()
+        orc.forward_projection(vo, vol, 0, i, False)
+        orc.compare(vo, projs[i], i)
+    t_fp = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for i in idx:
+        orc.back_projection(vo, vol, 0, i, float(p["sirt"]), img=projs[i].copy())
+    t_bp = time.perf_counter() - t0
+    t_ctf = ctf_time[0]
+    scale = ny / y_extent
+    per_proj = ((t_fp + t_bp - t_ctf) * scale + t_ctf) / len(idx)
+    vu = nx * ny * nz / per_proj
+    from oracle.lib import NTHREADS
+
+    return vu, dict(per_projection_s=per_proj, sample=f"{len(idx)} projections of the workload on a "
+                    f"{nx}x{y_extent}x{nz} tilt-axis slice (volume {nx}x{ny}x{nz}); voxel work x{scale:.0f}, "
+                    f"CTF chain (1024^2 FFTs) counted once", cores=NTHREADS)
+
+
+def run_reference(args):
+    ws, rank, _ = _dist_setup()
+    if rank != 0:
+        return 0
+    from artiatomi_b200.workloads import CONFIGS
+
+    params = CONFIGS[args.workload]
+    for _ in range(args.warmup):
+        cpu_sample(params, n_proj_sample=1)
+    vals = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        v, det = cpu_sample(params, n_proj_sample=2)
+        vals.append(v)
+    value = float(np.median(vals))
+    ms = params["dims"][0] * params["dims"][1] * params["dims"][2] * params["n_proj"] / value * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "volume": list(params["dims"]), "projections": params["n_proj"],
+                       "oversampling": params["os"], "sirt_count": params["sirt"], "ctf": params["ctf"]},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": det["cores"], "kind": "port",
+                             "sample": det["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_esb(args):
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = _dist_setup()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    torch.cuda.set_device(dev)
+
+    import artiatomi_b200 as E
+    from artiatomi_b200 import workloads as WL
+
+    params = dict(WL.CONFIGS[args.workload])
+    wl = WL.build(args.workload, params, seed=rank)
+    stream = torch.cuda.Stream()
+    rec = E.Reconstructor(wl.cfg, wl.pg, wl.tilt, wl.defocus, stream=stream)
+    vol = torch.zeros(params["dims"][::-1], dtype=torch.float32, device=dev)
+    sirt = params["sirt"]
+
+    def step(projs):
+        rec.sart(wl.vg, vol, projs, wl.index_list, iterations=1, sirt_count=sirt, volume_is_empty=False)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(wl.projections)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    rec.enable_timing(True)
+    rec.timing()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.steps):
+                step(wl.projections)
+            e1.record(stream)
+        torch.cuda.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    phases = rec.timing()
+    rec.enable_timing(False)
+    barrier()
+    t = torch.tensor([ms_total], device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = float(t.item()) / args.steps
+    vu_step = wl.voxel_updates_per_iteration
+    value = vu_step * ws / (ms_step * 1e-3)
+
+    # ---- end to end: host projections in, host volume out, every step
+    host_in = torch.empty(wl.projections.shape, dtype=torch.float32, pin_memory=True)
+    host_in.copy_(wl.projections.cpu())
+    host_out = torch.empty(vol.shape, dtype=torch.float32, pin_memory=True)
+    dev_in = torch.empty_like(wl.projections)
+    barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e2.record(stream)
+        for _ in range(args.steps):
+            dev_in.copy_(host_in, non_blocking=True)
+            step(dev_in)
+            host_out.copy_(vol, non_blocking=True)
+        e3.record(stream)
+    torch.cuda.synchronize()
+    t2 = torch.tensor([e2.elapsed_time(e3)], device=dev)
+    if ws > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t2.item()) / args.steps
+    e2e_value = vu_step * ws / (e2e_ms * 1e-3)
+
+    # ---- roofline of the dominant kernel (per projection of one step)
+    hbm, hbm_kind = _peaks()
+    V = wl.voxels
+    P = params["W"] * params["H"]
+    nproj = len(wl.index_list) * args.steps
+    fp_ms, fp_n = phases["fp"]
+    bp_ms, bp_n = phases["bp"]
+    if bp_ms >= fp_ms:
+        slabs = bp_n / nproj
+        bytes_unit = 2 * V * 4 + slabs * P * 4
+        name, t_unit, launches = "back-projection (all slab launches of one projection)", bp_ms / nproj, bp_n
+    else:
+        slabs = (fp_n / nproj) - 1
+        bytes_unit = V * 4 + (2 * slabs + 2) * P * 4
+        name, t_unit, launches = "forward projection (slicer launches + traversal length of one projection)", \
+            fp_ms / nproj, fp_n
+    achieved = bytes_unit / (t_unit * 1e-3) / 1e9
+    gpu_launches = sum(c for _, c in phases.values())
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, det = cpu_sample(params, n_proj_sample=1)
+        cpu = {"value": v, "unit": UNIT, "cores": det["cores"], "kind": "port", "sample": det["sample"]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid+bead phantom, "
+                "projections from this library's projector + noise)",
+                "config": {"workload": args.workload, "volume": list(params["dims"]),
+                           "projections": params["n_proj"], "projection_size": [params["W"], params["H"]],
+                           "oversampling": params["os"], "sirt_count": sirt, "ctf": params["ctf"],
+                           "ctf_slab_nm": 30.0, "voxel_storage": "f32",
+                           "l2": "inputs larger than L2 (volume 1 GiB)", "parallelism": f"replicas x{ws}"},
+                "e2e": {"value": e2e_value, "unit": UNIT,
+                        "h2d_bytes_per_step": int(wl.projections.numel() * 4),
+                        "d2h_bytes_per_step": int(vol.numel() * 4)},
+                "gpu_launches": int(gpu_launches),
+                "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm,
+                             "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
+                             "traffic": None, "algorithmic_bytes_per_unit": bytes_unit, "ms_per_unit": t_unit,
+                             "launches": launches},
+                "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
+                "clocks": clk.summary(),
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    rec.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["esb", "reference"], default="esb")
+    ap.add_argument("--workload", default="c2_sart_ctf")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_esb(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

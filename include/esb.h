@@ -1,0 +1,323 @@
+/*
+ * esb.h - C ABI of the B200 (sm_100a) EmSART reconstruction hot path.
+ *
+ * This header is the drop-in boundary. It replaces the reference's kernel
+ * wrappers (src/EmSART/Kernels.h:37-245), which launch named kernels from
+ * JIT-loaded PTX modules and pass geometry through __constant__ symbols that
+ * SetConstantValues writes by name (src/EmSART/Kernels.cpp:949-1131). Here
+ * the geometry travels as a plain struct (esb_constants). The volume is a
+ * linear device array of voxels in [z][y][x] order, with no CUDA array,
+ * texture or surface. Images are pitched device arrays of float.
+ *
+ * Conventions:
+ *  - Every function returns an int status: ESB_OK (0) on success, or one of
+ *    the ESB_ERR_* codes below. esb_last_error() then holds a message for the
+ *    calling thread. No C++ exception crosses this boundary (the reference
+ *    throws CudaException instead, CudaHelpers/CudaException.h:34-36).
+ *  - `stream` is a cudaStream_t passed as void*; NULL means the legacy
+ *    default stream. Launch functions are asynchronous. The reference's
+ *    wrappers synchronise after every launch and return the elapsed time
+ *    (Kernels.cpp:65-86).
+ *  - Pointers marked "device" must point to device memory of the current
+ *    device; pitches are in BYTES.
+ */
+#ifndef ESB_H
+#define ESB_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ESB_OK 0
+#define ESB_ERR_INVALID_ARGUMENT 1
+#define ESB_ERR_CUDA 2
+#define ESB_ERR_CUFFT 3
+#define ESB_ERR_UNSUPPORTED 4
+#define ESB_ERR_OUT_OF_MEMORY 5
+
+/* Voxel storage of the volume: FP32 (Volume<float>), FP16 (the reference's
+ * FP16Volume, Volume<unsigned short> over a HALF array, EmSart.cpp:404-414),
+ * or BF16 (added here). The arithmetic is always FP32. */
+#define ESB_VOXEL_F32 0
+#define ESB_VOXEL_F16 1
+#define ESB_VOXEL_BF16 2
+
+/* Everything SetConstantValues writes into the projector/back-projector
+ * modules (Kernels.cpp:949-1101; symbol list DeviceVariables.cuh:13-34). */
+typedef struct esb_constants {
+  float proj_norm[3];        /* c_projNorm   Projection::GetNormalVector  */
+  float detektor[3];         /* c_detektor   Projection::GetPosition      */
+  float u_pitch[3];          /* c_uPitch     Projection::GetPixelUPitch   */
+  float v_pitch[3];          /* c_vPitch     Projection::GetPixelVPitch   */
+  float bbox_min[3];         /* c_bBoxMin    Volume::GetSubVolumeBBoxMin  */
+  float bbox_max[3];         /* c_bBoxMax    Volume::GetSubVolumeBBoxMax  */
+  float bbox_rcp[3];         /* c_volumeBBoxRcp                           */
+  float volume_dim[3];       /* c_volumeDim  (sub-volume dimension)       */
+  float voxel_size[3];       /* c_voxelSize                               */
+  float z_shift;             /* c_zShiftForPartialVolume (0 for FP, Kernels.cpp:987) */
+  int volume_dim_x_quarter;  /* c_volumeDim_x_quarter = dim.x / 4         */
+  float detector_matrix[16]; /* c_DetectorMatrix (GetDetectorMatrix, os=1) */
+  float mag_aniso[9];        /* c_magAniso    3x3 row-major               */
+  float mag_aniso_inv[9];    /* c_magAnisoInv 3x3 row-major               */
+} esb_constants;
+
+/* Per-projection alignment as read from the marker file (MarkerFile items
+ * MFI_TiltAngle, MFI_X_Shift, MFI_Y_Shift, MFI_Magnifiaction,
+ * MFI_RotationPsi; MarkerFile.h:34-46) plus the config keys Projection reads
+ * (utils/Config.cpp:303-494). */
+typedef struct esb_tilt_config {
+  float add_tilt_angle;    /* AddTiltAngle    */
+  float add_tilt_x_angle;  /* AddTiltXAngle   */
+  int use_fix_psi_angle;   /* UseFixPsiAngle  */
+  float psi_angle;         /* PsiAngle        */
+  float phi_angle;         /* PhiAngle        */
+} esb_tilt_config;
+
+/* Detector frame of one projection, as the reference derives it. */
+typedef struct esb_proj_geom {
+  float detektor[3];
+  float u_pitch[3];
+  float v_pitch[3];
+  float proj_norm[3];
+  float detector_matrix[16];
+} esb_proj_geom;
+
+/* Placement of a (sub-)volume in space (Volume.cpp:27-306). */
+typedef struct esb_vol_geom {
+  float bbox_min[3];  /* sub-volume bbox min */
+  float bbox_max[3];  /* sub-volume bbox max */
+  float bbox_rcp[3];  /* 1 / (sub-volume dim * voxel size) */
+  float dim[3];       /* sub-volume dimension */
+  float voxel_size[3];
+  float z_shift;      /* Volume::GetSubVolumeZShift */
+  float full_dim[3];  /* whole-volume dimension */
+  float full_bbox_min[3];
+  float full_bbox_max[3];
+} esb_vol_geom;
+
+const char* esb_last_error(void);
+int esb_version(void);
+
+/* ---------------------------------------------------------------- geometry
+ * Host functions; no device work. */
+
+/* Projection::GetPosition / GetPixelUPitch / GetPixelVPitch /
+ * GetNormalVector / GetDetectorMatrix(os=1) (Projection.cpp:80-404) for every
+ * projection. extra_shift (2 floats per projection, may be NULL) is
+ * Projection::SetExtraShift (Projection.cpp:1102-1108). */
+int esb_projection_geometry(int n_proj, int width, int height, const float* tilt_deg, const float* x_shift,
+                            const float* y_shift, const float* magnification, const float* psi_deg,
+                            const float* extra_shift, const esb_tilt_config* cfg, esb_proj_geom* out);
+
+/* Volume(dim, subvol_count, subvol) + PositionInSpace(voxelSize, volumeShift,
+ * shiftXY=0) (Volume.cpp:82-114, 270-287), for sub-volume `subvol`. */
+int esb_volume_geometry(const int dim[3], int subvol_count, int subvol, const float voxel_size[3],
+                        const float volume_shift[3], esb_vol_geom* out);
+
+/* Volume::PositionInSpace for a particle box (Volume.cpp:289-306): a
+ * size^3 box of voxel size vs_sub centred on motive-list position pos
+ * (1-based) plus shift, inside the full volume `vol`. */
+int esb_subvolume_geometry(int size, float vs_sub, const esb_vol_geom* vol, const float pos[3],
+                           const float shift[3], esb_vol_geom* out);
+
+/* Reconstructor::GetMagAnistropyMatrix (Reconstructor.cpp:386-426). */
+int esb_mag_aniso_matrix(float amount, float angle_deg, float dim_x, float dim_y, float out[9]);
+
+/* SetConstantValues (Kernels.cpp:949-1101): assembles the kernel constants
+ * of projection `p` and sub-volume `v`. for_bp selects the BP variant, which
+ * sets c_zShiftForPartialVolume to the sub-volume's z shift; the FP variant
+ * sets 0. */
+int esb_set_constant_values(const esb_proj_geom* p, const esb_vol_geom* v, const float mag_aniso[9],
+                            const float mag_aniso_inv[9], int for_bp, esb_constants* out);
+
+/* Projection::ComputeHitPoints (Projection.cpp:850-1049): the volume's
+ * shadow corners pA..pD on the detector as 8 ints (x,y pairs). */
+int esb_compute_hit_points(const esb_proj_geom* p, const esb_vol_geom* v, int out[8]);
+
+/* Reconstructor::GetDefocusDistances (Reconstructor.cpp:53-173). */
+int esb_defocus_distances(const esb_proj_geom* p, const esb_vol_geom* v, int width, int height, float* t_in,
+                          float* t_out);
+
+/* Reconstructor::GetDefocusMinMax (Reconstructor.cpp:178-201). */
+int esb_defocus_min_max(float ray, float defocus_min_nm, float defocus_max_nm, float tilt_deg, float add_tilt_deg,
+                        float pixel_size_nm, float slice_thickness_nm, float volume_shift_z, int ignore_z_shift,
+                        int switch_direction, float* out_min, float* out_max);
+
+/* Projection::CreateProjectionIndexList (Projection.cpp:561-640). type:
+ * 0 PLT_NORMAL, 1 PLT_RANDOM, 2 PLT_RANDOM_START_ZERO_TILT. `good` marks the
+ * projections MarkerFile::CheckIfProjIndexIsGood accepts (NULL = all). Uses
+ * the C library's srand(0)/rand() as the reference does. Returns the count
+ * in *count; out holds n_proj ints. */
+int esb_projection_index_list(int type, int n_proj, const float* tilt_deg, const int* good, int* out, int* count);
+
+/* ------------------------------------------------------------ kernels
+ * One entry point per reference kernel wrapper. Device pointers. */
+
+/* FPKernel::operator() (Kernels.cpp:46-88) -> kernel `march`
+ * (ForwardProjectionRayMarcher_TL.cu:58-160). proj += line integral,
+ * dist = mean sub-ray chord, for pixels in [roi_x0,roi_x1) x [roi_y0,roi_y1). */
+int esb_fp(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj, float* dist,
+           size_t pitch, int roi_x0, int roi_y0, int roi_x1, int roi_y1, void* stream);
+
+/* SlicerKernel::operator() (Kernels.cpp:103-150) -> kernel `slicer`
+ * (ForwardProjectionSlicer.cu:57-220): proj += integral over t in [tmin,tmax]. */
+int esb_fp_slicer(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj,
+                  size_t pitch, float tmin, float tmax, int roi_x0, int roi_y0, int roi_x1, int roi_y1, void* stream);
+
+/* VolTravLengthKernel::operator() (Kernels.cpp:160-205) -> kernel
+ * `volTraversalLength` (ForwardProjectionSlicer.cu:224-288): dist += chord. */
+int esb_vol_traversal_length(const esb_constants* c, int proj_x, int proj_y, float* dist, size_t pitch, int roi_x0,
+                             int roi_y0, int roi_x1, int roi_y1, void* stream);
+
+/* CompKernel::operator() (Kernels.cpp:218-260) -> kernel `compare`
+ * (Compare.cu:50-130). virt <- tapered residual per unit length. */
+int esb_compare(int proj_x, int proj_y, size_t pitch, const float* real, float* virt, const float* dist,
+                float real_length, const float crop[4], const float crop_dim[4], float proj_val_scale, void* stream);
+
+/* CropBorderKernel::operator() (Kernels.cpp:276-318) -> kernel `cropBorder`
+ * (Compare.cu:171-277). p = pA..pD as (x,y) ints. */
+int esb_crop_border(int proj_x, int proj_y, size_t pitch, float* img, const float cut_length[2],
+                    const float dim_length[2], const int p[8], void* stream);
+
+/* BPKernel::operator() (Kernels.cpp:327-379) -> kernels `backProjection` /
+ * `backProjectionFP16` (BackProjectionSquareOS.cu:263-1291). vol +=
+ * lambda * sum(img*chord)/sum(chord) per voxel. Only 4-voxel quads whose
+ * first corner's depth lies in [dist_min, dist_max) are updated.
+ * linear_filter selects the bilinear sampling of CTF mode
+ * (Reconstructor.cpp:318-327). */
+int esb_bp(const esb_constants* c, void* vol, int voxel_type, int proj_x, int proj_y, const float* img, size_t pitch,
+           float lambda, int oversampling, float dist_min, float dist_max, int linear_filter, void* stream);
+
+/* CopyToSquareKernel::operator() (Kernels.cpp:808-850) -> `makeSquare`
+ * (CopyToSquare.cu:38-92); out is dense maxsize x maxsize. */
+int esb_make_square(int proj_x, int proj_y, size_t pitch, const float* in, int maxsize, float* out, int border_x,
+                    int border_y, int mirror_y, int fill_zero, void* stream);
+
+/* CTFKernel::operator() (Kernels.cpp:395-436) with the constants of
+ * SetConstantValues(CTFKernel...) (Kernels.cpp:1104-1131) -> `ctf`
+ * (ctf.cu:82-240), in place on the N/2+1 x N half spectrum. Units as the
+ * reference's callers use them: defocus in nm, angle in degrees, pixel size
+ * in nm, Cs in mm, voltage in kV. amp_contrast is fixed to 0 by the
+ * reference; it is exposed here. */
+int esb_ctf(float* spectrum, int n, float defocus_min_nm, float defocus_max_nm, float angle_deg, int apply_for_fp,
+            int phase_flip_only, float wiener_noise_level, const float beta_fac[4], float cs_mm, float voltage_kv,
+            float amp_contrast, float pixel_size_nm, void* stream);
+
+/* WbpWeightingKernel::operator() (Kernels.cpp:453-490) -> `wbpWeighting`
+ * (wbpWeighting.cu:50-144). filter: 0 RAMP, 1 EXACT, 2 CONTRAST2,
+ * 3 CONTRAST10, 4 CONTRAST30. */
+int esb_wbp_weighting(float* spectrum, int n, float psi_deg, int filter, void* stream);
+
+/* FourFilterKernel (Kernels.cpp:504-540) -> `fourierFilter` (wbpWeighting.cu:148-212). */
+int esb_fourier_filter(float* spectrum, int n, float lp, float hp, float lps, float hps, void* stream);
+
+/* DoseWeightingKernel (Kernels.cpp:556-590) -> `doseWeighting` (wbpWeighting.cu:216-240). */
+int esb_dose_weighting(float* spectrum, int n, float dose, float pixel_size_a, void* stream);
+
+/* ConvVol3DKernel (Kernels.cpp:1180-1230) -> `convertVolume3DFP16ToFP32`
+ * (BackProjectionSquareOS.cu:1326-1355): out = -vol as float. Also accepts
+ * FP32 and BF16 storage. */
+int esb_convert_volume(const void* vol, int voxel_type, long n_voxels, float* out, int negate, void* stream);
+
+/* Store a float volume into the given voxel type (round to nearest even). */
+int esb_store_volume(const float* in, long n_voxels, void* vol, int voxel_type, void* stream);
+
+/* ----------------------------------------------------- reconstructor
+ * Reconstructor (Reconstructor.h:181-249) and the EmSART driver loops. The
+ * object owns its device buffers (proj_d, dist_d, realproj_d, the padded
+ * square image, the half spectrum) and its cuFFT plans, like the
+ * reference's Reconstructor (Reconstructor.cpp:203-372). */
+
+typedef struct esb_recon_config {
+  int proj_x, proj_y;             /* projection size */
+  int n_proj;
+  float lambda;                   /* Lambda */
+  int oversampling;               /* OverSampling */
+  int ctf_mode;                   /* CtfMode */
+  float cut_length[2];            /* CutLength */
+  float dim_length[2];            /* DimLength */
+  float crop[4];                  /* Crop */
+  float crop_dim[4];              /* CropDim */
+  float projection_scale_factor;  /* ProjectionScaleFactor */
+  float pixel_size_nm;            /* projection pixel size in nm */
+  float cs_mm, voltage_kv, amp_contrast;  /* Cs, Voltage; ampContrast (0 in the reference) */
+  float ctf_slice_thickness_nm;   /* CTFSliceThickness */
+  float ctf_beta_fac[4];          /* CTFBetaFac */
+  float wiener_noise_level;       /* WienerFilterNoiseLevel */
+  int phase_flip_only;            /* PhaseFlipOnly */
+  int ignore_z_shift_for_ctf;     /* IgnoreZShiftForCTF */
+  int switch_ctf_direction;       /* SwitchCTFDirectionForIMOD */
+  float volume_shift[3];          /* VolumeShift */
+  float add_tilt_angle;           /* AddTiltAngle */
+} esb_recon_config;
+
+typedef struct esb_reconstructor esb_reconstructor;
+
+/* geoms/tilt_deg: per projection; defocus: per projection (min nm, max nm,
+ * astigmatism angle deg) or NULL without CTF; mag_aniso/inv: 3x3 each. */
+int esb_reconstructor_create(const esb_recon_config* cfg, const esb_proj_geom* geoms, const float* tilt_deg,
+                             const float* defocus, const float mag_aniso[9], const float mag_aniso_inv[9],
+                             esb_reconstructor** out);
+int esb_reconstructor_destroy(esb_reconstructor* rec);
+int esb_reconstructor_set_stream(esb_reconstructor* rec, void* stream);
+/* Device pointers to the reconstructor's W x H float images (pitch W*4). */
+int esb_reconstructor_buffers(esb_reconstructor* rec, float** proj_d, float** dist_d, float** real_d);
+
+/* Per-phase device timing of the reconstructor's launches (CUDA events on
+ * its stream); the reference times every wrapper launch synchronously and
+ * returns ms (Kernels.cpp:65-86). Phases: 0 forward projection kernels,
+ * 1 back-projection kernel, 2 CTF chain (pad, FFTs, filter, crop),
+ * 3 compare and buffer resets. esb_reconstructor_timing synchronises the
+ * stream, returns the summed ms and launch counts since the previous call,
+ * and restarts the accumulation. */
+int esb_reconstructor_enable_timing(esb_reconstructor* rec, int enable);
+int esb_reconstructor_timing(esb_reconstructor* rec, double out_ms[4], int counts[4]);
+
+/* ResetProjectionsDevice (Reconstructor.cpp:1678-1682). */
+int esb_rec_reset_projections(esb_reconstructor* rec);
+/* ForwardProjection (Reconstructor.cpp:1411-1421), CTF or not. */
+int esb_rec_forward_projection(esb_reconstructor* rec, const esb_vol_geom* vg, const void* vol, int voxel_type,
+                               int index, int volume_is_empty);
+/* Compare (Reconstructor.cpp:1386-1405). real: device image W x H. */
+int esb_rec_compare(esb_reconstructor* rec, const esb_vol_geom* vg, const float* real, int index);
+/* BackProjection (Reconstructor.cpp:871-887 / 920-969) of proj_d. */
+int esb_rec_back_projection(esb_reconstructor* rec, const esb_vol_geom* vg, void* vol, int voxel_type, int index,
+                            float sirt_count);
+
+/* The SART driver loop of EmSart.cpp:579-675 for one GPU: iterations x
+ * ordered subsets of sirt_count projections x {FP, compare} then {BP}.
+ * projections: device, n_proj images of W x H (already prepared);
+ * index_list: the projection order (esb_projection_index_list);
+ * *volume_is_empty: in/out flag of EmSart.cpp:425,653. */
+int esb_sart_run(esb_reconstructor* rec, const esb_vol_geom* vg, void* vol, int voxel_type, const float* projections,
+                 const int* index_list, int proj_count, int iterations, int sirt_count, int* volume_is_empty);
+
+/* The sub-volume reconstruction of EmSartSubVolumes.cpp:611-705 with
+ * Reconstructor::BackProjection(vol, subVolumes, ...)
+ * (Reconstructor.cpp:893-1033): weighted back-projection (lambda = 1) of
+ * n_particles boxes from the prepared (WBP-weighted) projections.
+ *   full_vol   - placement of the whole tomogram (CTF slabs are cut on it)
+ *   sub_geoms  - per particle placement (esb_subvolume_geometry); boxes may
+ *                differ in size
+ *   pair_geoms - [n_particles][n_proj] detector frames including the
+ *                particle's per-tilt extra shift (esb_projection_geometry
+ *                with extra_shift; Projection::SetExtraShift)
+ *   active     - [n_particles][n_proj] 0/1, or NULL for all: the reference
+ *                skips a tilt whose |shift| >= MaxShift - 0.5
+ *                (EmSartSubVolumes.cpp:651-662)
+ *   boxes      - per particle device pointer to a FP32 box, accumulated into
+ *   projections- device, n_proj prepared images of W x H
+ * batched = 0: one launch per particle per tilt (the reference's scheme);
+ * batched = 1: one launch per tilt covering every particle. */
+int esb_subvolume_wbp(esb_reconstructor* rec, const esb_vol_geom* full_vol, int n_particles,
+                      const esb_vol_geom* sub_geoms, const esb_proj_geom* pair_geoms, const unsigned char* active,
+                      float* const* boxes, const float* projections, const int* index_list, int proj_count,
+                      int batched);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ESB_H */
