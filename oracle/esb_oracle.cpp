@@ -469,9 +469,26 @@ void bp_quad(const OrcGeom& g, void* volData, int dtype, int qx, int y, int z, c
 }
 
 // ------------------------------------------------------------------ FFT
-// Iterative radix-2 complex FFT in double (power-of-two N), sign -1 forward.
+// Complex DFT in double, sign -1 forward: iterative radix-2 for power-of-two
+// lengths, direct O(n^2) summation otherwise (the oracle's sizes are small
+// when they are not powers of two).
 using cd = std::complex<double>;
+void dft_direct(cd* a, int n, int sign) {
+  std::vector<cd> out(n), tw(n);
+  for (int k = 0; k < n; ++k) tw[k] = cd(std::cos(sign * 2.0 * M_PI * k / n), std::sin(sign * 2.0 * M_PI * k / n));
+  for (int k = 0; k < n; ++k) {
+    cd s(0);
+    for (int j = 0; j < n; ++j) s += a[j] * tw[(long)j * k % n];
+    out[k] = s;
+  }
+  for (int k = 0; k < n; ++k) a[k] = out[k];
+}
+
 void fft1d(cd* a, int n, int sign) {
+  if (n & (n - 1)) {
+    dft_direct(a, n, sign);
+    return;
+  }
   for (int i = 1, j = 0; i < n; ++i) {
     int bit = n >> 1;
     for (; j & bit; bit >>= 1) j ^= bit;
@@ -525,10 +542,9 @@ void c2r_2d(const std::complex<float>* in, float* out, int n, int nthreads) {
   parallel_for(n, nthreads, [&](int y) {
     std::vector<cd> row(n);
     for (int x = 0; x < nh; ++x) row[x] = tmp[(size_t)y * n + x];
-    // X(N-x) = conj of the spectrum at (N-x) mirrored in y as well; after the
-    // y transform the row is Hermitian in x: X(y, N-x) = conj(X(-y, x)).
-    int ym = (n - y) % n;
-    for (int x = nh; x < n; ++x) row[x] = std::conj(tmp[(size_t)ym * n + (n - x)]);
+    // The full spectrum obeys X(ky, N-kx) = conj(X(-ky, kx)); after the
+    // inverse transform along y this becomes Z(y, N-kx) = conj(Z(y, kx)).
+    for (int x = nh; x < n; ++x) row[x] = std::conj(tmp[(size_t)y * n + (n - x)]);
     fft1d(row.data(), n, +1);
     for (int x = 0; x < n; ++x) out[(size_t)y * n + x] = (float)row[x].real();
   });

@@ -81,8 +81,10 @@ def test_forward_and_back_projection_ctf():
         rec.forward_projection(case["vg"], vol_d, i, False)
         orc.reset()
         orc.forward_projection(case["vo"], case["vol"], 0, i, False)
-        assert rel_l2(host(proj_v), orc.proj) <= 1e-4, (i, rel_l2(host(proj_v), orc.proj))
-        assert rel_l2(host(dist_v), orc.dist) <= 1e-6
+        e = rel_l2(host(proj_v), orc.proj)
+        assert e <= 1e-4, (i, e)
+        e = rel_l2(host(dist_v), orc.dist)
+        assert e <= 1e-6, (i, e)
     # CTF back projection of a random residual
     vol_b = cuda(np.zeros(case["vol"].shape, np.float32))
     vo = np.zeros(case["vol"].shape, np.float32)
@@ -91,7 +93,8 @@ def test_forward_and_back_projection_ctf():
         proj_v.copy_(cuda(res))
         rec.back_projection(case["vg"], vol_b, i, 2.0)
         orc.back_projection(case["vo"], vo, 0, i, 2.0, img=res.copy())
-    assert rel_l2(host(vol_b), vo) <= 1e-4
+    e = rel_l2(host(vol_b), vo)
+    assert e <= 1e-4, e
 
 
 def test_sart_ctf():
@@ -113,7 +116,8 @@ def test_sart_ctf():
     orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], defocus, precision=0)
     vo = np.zeros(case["vol"].shape, np.float32)
     orc.sart(case["vo"], vo, 0, projs, il, 2, 2)
-    assert rel_l2(host(vol_d), vo) <= 1e-4
+    e = rel_l2(host(vol_d), vo)
+    assert e <= 1e-4, e
 
 
 @pytest.mark.parametrize("ctf,batched", [(False, False), (False, True), (True, True)])
@@ -160,5 +164,6 @@ def test_subvolume_wbp(ctf, batched):
     bo = [np.zeros((s, s, s), np.float32) for s in sizes]
     orc.subvolume_wbp(fo, subo, pair_o, bo, projs, il, active=active)
     for b, o in zip(boxes, bo):
-        assert rel_l2(host(b), o) <= (1e-4 if ctf else 1e-5)
+        e = rel_l2(host(b), o)
+        assert e <= (1e-4 if ctf else 1e-5), e
         assert np.abs(o).sum() > 0
