@@ -1,6 +1,9 @@
 """Build libesb.so (the sm_100a CUDA library behind include/esb.h) in-tree.
 
-Usage: python -m artiatomi_b200.build [--force]
+Usage: python artiatomi_b200/build.py [--force]
+
+(Run it as a file: importing the package loads libesb.so, which is what this
+script builds.)
 
 The library is compiled with nvcc for sm_100a only and linked against cuFFT.
 The projector/back-projector translation unit is compiled with --fmad=false
@@ -49,6 +52,7 @@ def _stale(target: Path, deps) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
+    force_link = False
     headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "esb.h"]
     objs = []
     for src, extra in UNITS:
@@ -57,15 +61,18 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             continue
         o = BUILD / (s.stem + ".o")
         objs.append(o)
-        if force or _stale(o, [s] + headers):
-            cmd = [nvcc(), *ARCH, *COMMON, *extra, "-I", str(PKG.parent / "include"), "-c", str(s), "-o", str(o)]
-            if s.suffix == ".cpp":
-                cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-I", str(PKG.parent / "include"), "-c", str(s),
-                       "-o", str(o)]
+        cmd = [nvcc(), *ARCH, *COMMON, *extra, "-I", str(PKG.parent / "include"), "-c", str(s), "-o", str(o)]
+        if s.suffix == ".cpp":
+            cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-I", str(PKG.parent / "include"), "-c", str(s), "-o", str(o)]
+        stamp = o.with_suffix(".cmd")
+        flags_changed = not stamp.exists() or stamp.read_text() != " ".join(cmd)
+        if force or flags_changed or _stale(o, [s] + headers):
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
-    if force or _stale(OUT, objs):
+            stamp.write_text(" ".join(cmd))
+            force_link = True
+    if force or force_link or _stale(OUT, objs):
         # cudart is linked statically (nvcc's default); cuFFT from the toolkit,
         # found through the rpath so that another cuFFT in the process (torch's)
         # is not picked up by accident.
