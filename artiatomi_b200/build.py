@@ -32,6 +32,7 @@ UNITS = [
     ("esb_projector_fast.cu", []),
     ("esb_image.cu", ["--fmad=false"]),
     ("esb_api.cu", []),
+    ("esb_noalloc.cu", []),
     ("esb_geometry.cpp", []),
 ]
 

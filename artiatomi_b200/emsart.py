@@ -237,6 +237,27 @@ def store_volume(src, vol, stream=None) -> None:
     check(lib.esb_store_volume(fptr(src), src.numel(), fptr(vol), _voxel_type_of(vol), _stream(stream)))
 
 
+def sart_projection_update_noalloc(cfg: "ReconConfig", pg, vg, vol, real, sirt_count: float = 1.0,
+                                   volume_is_empty: bool = False, mag=None, mag_inv=None, stream=None) -> None:
+    """One SART update of `vol` from projection geometry `pg` and measured
+    image `real` (no CTF), allocating no device memory.
+
+    For callers that cannot call cudaMalloc (device memory owned and budgeted
+    by their own allocator, no allocation after start-up, no implicit device
+    synchronisation in the loop). The two scratch images live in a fixed
+    32 MiB array inside the library (projections up to 2048 x 2048 pixels),
+    shared by all calls: overlapping calls on the GPU race, and the first call
+    on a device, which looks up the array's address, should come before any
+    stream capture. Same result as Reconstructor.reset_projections /
+    forward_projection / compare / back_projection.
+    """
+    m = _f32(IDENTITY3 if mag is None else mag, 9)
+    mi = _f32(IDENTITY3 if mag_inv is None else mag_inv, 9)
+    check(lib.esb_sart_projection_update_noalloc(C.byref(cfg.c()), C.byref(pg), C.byref(vg), fptr(m), fptr(mi),
+                                                 fptr(vol), _voxel_type_of(vol), fptr(real), sirt_count,
+                                                 int(volume_is_empty), _stream(stream)))
+
+
 class _CudaArray:
     def __init__(self, address: int, shape, typestr: str = "<f4"):
         self.__cuda_array_interface__ = {"data": (int(address), False), "shape": tuple(shape), "typestr": typestr,

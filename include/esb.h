@@ -316,6 +316,35 @@ int esb_subvolume_wbp(esb_reconstructor* rec, const esb_vol_geom* full_vol, int 
                       float* const* boxes, const float* projections, const int* index_list, int proj_count,
                       int batched);
 
+/* ------------------------------------------------ no-allocation variant
+ * No counterpart in the reference. One SART update of `vol` from one
+ * projection without CTF: the sequence esb_rec_reset_projections,
+ * esb_rec_forward_projection, esb_rec_compare and esb_rec_back_projection
+ * perform on a reconstructor. This entry point allocates no device memory,
+ * for callers that cannot call cudaMalloc: applications whose device memory
+ * is owned and budgeted by their own allocator, processes that must not
+ * allocate after start-up, and loops that must not pay cudaMalloc's implicit
+ * device synchronisation.
+ *  - Its two scratch images (forward projection and ray lengths) live in a
+ *    fixed array inside the library of 2 x ESB_NOALLOC_MAX_PIXELS floats
+ *    (32 MiB). The array stays resident on every GPU that loads it, until the
+ *    process exits. Projections larger than ESB_NOALLOC_MAX_PIXELS pixels are
+ *    rejected with ESB_ERR_INVALID_ARGUMENT.
+ *  - The first call on a device looks up the array's device address (set-up,
+ *    once per device). Make that first call before any stream capture.
+ *  - Every call shares the one array, and the array keeps the previous call's
+ *    images; each call clears them first. Calls that overlap on the GPU (on
+ *    different streams, or on different host threads, to the same device)
+ *    race on the array and must be serialised by the caller.
+ *  - cfg->ctf_mode must be 0 (the CTF chain needs FFT plans, which allocate).
+ *  - real: device W x H image (pitch W*4). pg/vg/mag_aniso: as for
+ *    esb_set_constant_values. */
+#define ESB_NOALLOC_MAX_PIXELS (2048 * 2048)
+int esb_sart_projection_update_noalloc(const esb_recon_config* cfg, const esb_proj_geom* pg, const esb_vol_geom* vg,
+                                       const float mag_aniso[9], const float mag_aniso_inv[9], void* vol,
+                                       int voxel_type, const float* real, float sirt_count, int volume_is_empty,
+                                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif
