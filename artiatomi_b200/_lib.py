@@ -53,7 +53,9 @@ class ReconConfig(C.Structure):
                 ("voltage_kv", C.c_float), ("amp_contrast", C.c_float), ("ctf_slice_thickness_nm", C.c_float),
                 ("ctf_beta_fac", f4), ("wiener_noise_level", C.c_float), ("phase_flip_only", C.c_int),
                 ("ignore_z_shift_for_ctf", C.c_int), ("switch_ctf_direction", C.c_int), ("volume_shift", f3),
-                ("add_tilt_angle", C.c_float)]
+                ("add_tilt_angle", C.c_float), ("variant", C.c_int)]
+
+VARIANT_FAITHFUL, VARIANT_FAST = 0, 1
 
 
 P = C.c_void_p
@@ -79,6 +81,9 @@ _SIGS = {
     "esb_compare": ([I, I, SZ, P, P, P, F, P, P, F, P], I),
     "esb_crop_border": ([I, I, SZ, P, P, P, P, P], I),
     "esb_bp": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, I, F, F, I, P], I),
+    "esb_fp_fast": ([C.POINTER(Constants), P, I, I, I, P, P, SZ, I, I, I, I, P], I),
+    "esb_fp_slicer_fast": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, F, I, I, I, I, P], I),
+    "esb_bp_fast": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, I, F, F, I, P], I),
     "esb_make_square": ([I, I, SZ, P, I, P, I, I, I, I, P], I),
     "esb_ctf": ([P, I, F, F, F, I, I, F, P, F, F, F, F, P], I),
     "esb_wbp_weighting": ([P, I, F, I, P], I),

@@ -30,6 +30,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("esb_projector.cu", ["--fmad=false"]),
     ("esb_projector_fast.cu", []),
+    ("esb_backprojector_fast.cu", []),
     ("esb_image.cu", ["--fmad=false"]),
     ("esb_api.cu", []),
     ("esb_noalloc.cu", []),

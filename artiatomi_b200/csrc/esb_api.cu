@@ -21,6 +21,15 @@ cudaError_t launch_slicer(const KConst& c, const void* vol, int vt, float* proj,
 cudaError_t launch_travlen(const KConst& c, float* dist, size_t pitchE, int x0, int y0, int x1, int y1, cudaStream_t st);
 cudaError_t launch_bp(const KConst& c, void* vol, int vt, const float* img, int pw, int ph, size_t pitchE, float lambda,
                       int os, float distMin, float distMax, int linear, cudaStream_t st);
+cudaError_t launch_project_fast(const KConst& c, const void* vol, int vt, int mode, float* proj, float* dist,
+                                size_t pitchE, float tmin, float tmax, int x0, int y0, int x1, int y1, cudaStream_t st);
+cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img, int pw, int ph, size_t pitchE,
+                           float lambda, int os, float distMin, float distMax, int linear, cudaStream_t st);
+cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
+                                 const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
+                                 float distMin, float distMax, int linear, cudaStream_t st);
+cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float* imgs, size_t img_stride,
+                                size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1, cudaStream_t st);
 cudaError_t launch_compare(int pw, int ph, size_t pitchE, const float* real, float* virt, const float* dist,
                            float realLength, float4 cut, float4 dim, float scale, cudaStream_t st);
 cudaError_t launch_crop_border(int pw, int ph, size_t pitchE, float* img, float2 cut, float2 dim, const int* p,
@@ -172,6 +181,50 @@ int esb_bp(const esb_constants* c, void* vol, int voxel_type, int proj_x, int pr
   return ok();
 }
 
+int esb_fp_fast(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj,
+                float* dist, size_t pitch, int roi_x0, int roi_y0, int roi_x1, int roi_y1, void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_fp_fast")) || (r = check_image(proj_x, proj_y, pitch, "esb_fp_fast"))) return r;
+  if (!vol || !proj || !dist || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_fp_fast: invalid argument");
+  roi_x0 = roi_x0 < 0 ? 0 : roi_x0;
+  roi_y0 = roi_y0 < 0 ? 0 : roi_y0;
+  roi_x1 = roi_x1 > proj_x ? proj_x : roi_x1;
+  roi_y1 = roi_y1 > proj_y ? proj_y : roi_y1;
+  ESB_CK(launch_project_fast(to_kconst(*c), vol, voxel_type, 0, proj, dist, pitch / 4, 0.f, 0.f, roi_x0, roi_y0, roi_x1,
+                             roi_y1, as_stream(stream)), "esb_fp_fast");
+  return ok();
+}
+
+int esb_fp_slicer_fast(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj,
+                       size_t pitch, float tmin, float tmax, int roi_x0, int roi_y0, int roi_x1, int roi_y1,
+                       void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_fp_slicer_fast")) || (r = check_image(proj_x, proj_y, pitch, "esb_fp_slicer_fast")))
+    return r;
+  if (!vol || !proj || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_fp_slicer_fast: invalid argument");
+  roi_x0 = roi_x0 < 0 ? 0 : roi_x0;
+  roi_y0 = roi_y0 < 0 ? 0 : roi_y0;
+  roi_x1 = roi_x1 > proj_x ? proj_x : roi_x1;
+  roi_y1 = roi_y1 > proj_y ? proj_y : roi_y1;
+  ESB_CK(launch_project_fast(to_kconst(*c), vol, voxel_type, 1, proj, nullptr, pitch / 4, tmin, tmax, roi_x0, roi_y0,
+                             roi_x1, roi_y1, as_stream(stream)), "esb_fp_slicer_fast");
+  return ok();
+}
+
+int esb_bp_fast(const esb_constants* c, void* vol, int voxel_type, int proj_x, int proj_y, const float* img,
+                size_t pitch, float lambda, int oversampling, float dist_min, float dist_max, int linear_filter,
+                void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_bp_fast")) || (r = check_image(proj_x, proj_y, pitch, "esb_bp_fast"))) return r;
+  if (!vol || !img || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_bp_fast: invalid argument");
+  if (oversampling < 1) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_bp_fast: oversampling must be >= 1");
+  if (4 * c->volume_dim_x_quarter > (int)c->volume_dim[0])
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_bp_fast: volume_dim_x_quarter exceeds volume_dim.x / 4");
+  ESB_CK(launch_bp_fast(to_kconst(*c), vol, voxel_type, img, proj_x, proj_y, pitch / 4, lambda, oversampling, dist_min,
+                        dist_max, linear_filter, as_stream(stream)), "esb_bp_fast");
+  return ok();
+}
+
 int esb_make_square(int proj_x, int proj_y, size_t pitch, const float* in, int maxsize, float* out, int border_x,
                     int border_y, int mirror_y, int fill_zero, void* stream) {
   int r;
@@ -281,6 +334,8 @@ struct esb_reconstructor {
   CtfConst ctfk;
   bool timing = false;
   PhaseTimer timers[4];
+  float* slab_imgs = nullptr;  // per-slab images of the fused CTF paths
+  size_t slab_cap = 0;         // capacity in images
 };
 
 // Brackets a phase of launches with events when timing is enabled.
@@ -326,6 +381,9 @@ static void rec_free(esb_reconstructor* r) {
     cufftDestroy(r->c2r);
   }
   for (auto& t : r->timers) t.destroy();
+  cudaFree(r->slab_imgs);
+  r->slab_imgs = nullptr;
+  r->slab_cap = 0;
 }
 
 extern "C" {
@@ -427,6 +485,28 @@ int esb_rec_reset_projections(esb_reconstructor* r) {
 
 }  // extern "C"
 
+// Kernel variant of the reconstructor (faithful or fast).
+static cudaError_t rec_march(esb_reconstructor* r, const KConst& c, const void* vol, int vt) {
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y;
+  if (r->cfg.variant == ESB_VARIANT_FAST)
+    return launch_project_fast(c, vol, vt, 0, r->proj_d, r->dist_d, W, 0.f, 0.f, 0, 0, W, H, r->stream);
+  return launch_march(c, vol, vt, r->proj_d, r->dist_d, W, 0, 0, W, H, r->stream);
+}
+static cudaError_t rec_slicer(esb_reconstructor* r, const KConst& c, const void* vol, int vt, float* out, float t0,
+                              float t1) {
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y;
+  if (r->cfg.variant == ESB_VARIANT_FAST)
+    return launch_project_fast(c, vol, vt, 1, out, nullptr, W, t0, t1, 0, 0, W, H, r->stream);
+  return launch_slicer(c, vol, vt, out, W, t0, t1, 0, 0, W, H, r->stream);
+}
+static cudaError_t rec_bp(esb_reconstructor* r, const KConst& c, void* vol, int vt, const float* img, float lambda,
+                          float dmin, float dmax, int linear) {
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y;
+  if (r->cfg.variant == ESB_VARIANT_FAST)
+    return launch_bp_fast(c, vol, vt, img, W, H, W, lambda, r->cfg.oversampling, dmin, dmax, linear, r->stream);
+  return launch_bp(c, vol, vt, img, W, H, W, lambda, r->cfg.oversampling, dmin, dmax, linear, r->stream);
+}
+
 static int rec_check(esb_reconstructor* r, const esb_vol_geom* vg, int index, const char* where) {
   if (!r || !vg) return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": NULL argument");
   if (index < 0 || index >= r->cfg.n_proj) return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": index out of range");
@@ -461,6 +541,35 @@ static int rec_ctf_chain(esb_reconstructor* r, float* img, int crop_in, const in
   return ESB_OK;
 }
 
+// Slab boundaries of projection `index`: the reference's loop
+// for (ray = t_in; ray < t_out; ray += thickness/pixelsize) with its float
+// recurrence (Reconstructor.cpp:515, 935).
+static int rec_slab_table(esb_reconstructor* r, const esb_vol_geom* vg, int index, SlabTable& T) {
+  float t_in, t_out;
+  esb_defocus_distances(&r->geoms[index], vg, r->cfg.proj_x, r->cfg.proj_y, &t_in, &t_out);
+  const float step = r->cfg.ctf_slice_thickness_nm / r->cfg.pixel_size_nm;
+  int K = 0;
+  float ray = t_in;
+  for (; ray < t_out; ray += step) {
+    if (K >= ESB_MAX_SLABS) return fail(ESB_ERR_UNSUPPORTED, "more than 256 CTF slabs in one projection");
+    T.bound[K++] = ray;
+  }
+  T.bound[K] = ray;  // = bound[K-1] + step, the last slab's upper limit
+  T.count = K;
+  return ESB_OK;
+}
+
+static int rec_slab_capacity(esb_reconstructor* r, int count) {
+  if ((size_t)count <= r->slab_cap) return ESB_OK;
+  cudaFree(r->slab_imgs);
+  r->slab_imgs = nullptr;
+  r->slab_cap = 0;
+  const size_t bytes = (size_t)count * r->cfg.proj_x * r->cfg.proj_y * sizeof(float);
+  ESB_CK(cudaMalloc(&r->slab_imgs, bytes), "slab images");
+  r->slab_cap = count;
+  return ESB_OK;
+}
+
 extern "C" {
 
 int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, const void* vol, int voxel_type, int index,
@@ -478,7 +587,7 @@ int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, con
   }
   if (!cf.ctf_mode) {  // ForwardProjectionNoCTF (Reconstructor.cpp:429-438)
     PhaseScope ps(r, 0);
-    ESB_CK(launch_march(c, vol, voxel_type, r->proj_d, r->dist_d, W, 0, 0, W, H, r->stream), "esb_rec_forward_projection");
+    ESB_CK(rec_march(r, c, vol, voxel_type), "esb_rec_forward_projection");
     return ok();
   }
   // ForwardProjectionCTF (Reconstructor.cpp:496-590)
@@ -486,7 +595,32 @@ int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, con
   esb_defocus_distances(&r->geoms[index], vg, W, H, &t_in, &t_out);
   const float step = cf.ctf_slice_thickness_nm / cf.pixel_size_nm;
   const int full[8] = {0, H - 1, W - 1, H - 1, 0, 0, W - 1, 0};  // pA, pB, pC, pD (Reconstructor.cpp:559-566)
-  for (float ray = t_in; ray < t_out; ray += step) {
+  if (cf.variant == ESB_VARIANT_FAST) {
+    // all slabs in one slicer launch, then the CTF chain per slab image
+    SlabTable T;
+    if ((rc = rec_slab_table(r, vg, index, T))) return rc;
+    if ((rc = rec_slab_capacity(r, T.count))) return rc;
+    const size_t img = (size_t)W * H;
+    {
+      PhaseScope ps(r, 3);
+      ESB_CK(cudaMemsetAsync(r->slab_imgs, 0, (size_t)T.count * img * sizeof(float), r->stream),
+             "esb_rec_forward_projection");
+    }
+    {
+      PhaseScope ps(r, 0);
+      ESB_CK(launch_slicer_fused(c, vol, voxel_type, r->slab_imgs, img, W, T, 0, 0, W, H, r->stream),
+             "esb_rec_forward_projection");
+    }
+    for (int k = 0; k < T.count; ++k) {
+      float dmin, dmax;
+      esb_defocus_min_max(T.bound[k], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
+                          cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
+                          cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
+      if ((rc = rec_ctf_chain(r, r->slab_imgs + k * img, 1, full, index, dmin, dmax, 1, nullptr, r->proj_d, 1, full)))
+        return rc;
+    }
+  }
+  for (float ray = t_in; cf.variant != ESB_VARIANT_FAST && ray < t_out; ray += step) {
     float dmin, dmax;
     esb_defocus_min_max(ray, r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index], cf.add_tilt_angle,
                         cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2], cf.ignore_z_shift_for_ctf,
@@ -497,8 +631,7 @@ int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, con
     }
     {
       PhaseScope ps(r, 0);
-      ESB_CK(launch_slicer(c, vol, voxel_type, r->dist_d, W, ray, ray + step, 0, 0, W, H, r->stream),
-             "esb_rec_forward_projection");
+      ESB_CK(rec_slicer(r, c, vol, voxel_type, r->dist_d, ray, ray + step), "esb_rec_forward_projection");
     }
     if ((rc = rec_ctf_chain(r, r->dist_d, 1, full, index, dmin, dmax, 1, nullptr, r->proj_d, 1, full))) return rc;
   }
@@ -547,14 +680,33 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
                                 make_float2(cf.dim_length[0], cf.dim_length[1]), p, r->stream), "back projection");
     }
     PhaseScope ps(r, 1);
-    ESB_CK(launch_bp(c, vol, voxel_type, img, W, H, W, lambda, cf.oversampling, 0.0f, 9999999999999.0f, 0, r->stream),
-           "back projection");
+    ESB_CK(rec_bp(r, c, vol, voxel_type, img, lambda, 0.0f, 9999999999999.0f, 0), "back projection");
     return ESB_OK;
   }
   float t_in, t_out;
   esb_defocus_distances(&r->geoms[index], vg, W, H, &t_in, &t_out);
   const float step = cf.ctf_slice_thickness_nm / cf.pixel_size_nm;
   int rc;
+  if (cf.variant == ESB_VARIANT_FAST) {
+    // Wiener-filtered image per slab, then one back-projection launch that
+    // picks each quad's slab image by its first-corner depth
+    SlabTable T;
+    if ((rc = rec_slab_table(r, vg, index, T))) return rc;
+    if ((rc = rec_slab_capacity(r, T.count))) return rc;
+    const size_t npx = (size_t)W * H;
+    for (int k = 0; k < T.count; ++k) {
+      float dmin, dmax;
+      esb_defocus_min_max(T.bound[k], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
+                          cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
+                          cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
+      // cropBorder(proj_d) is re-applied to the residual on every slab (:954)
+      if ((rc = rec_ctf_chain(r, img, 1, p, index, dmin, dmax, 0, r->slab_imgs + k * npx, nullptr, 1, p))) return rc;
+    }
+    PhaseScope ps(r, 1);
+    ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, npx, T, W, H, W, lambda, cf.oversampling, 0.f, 0.f,
+                                1, r->stream), "back projection");
+    return ESB_OK;
+  }
   for (float ray = t_in; ray < t_out; ray += step) {
     float dmin, dmax;
     esb_defocus_min_max(ray, r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index], cf.add_tilt_angle,
@@ -563,8 +715,7 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
     // cropBorder(proj_d) is re-applied to the residual on every slab (:954)
     if ((rc = rec_ctf_chain(r, img, 1, p, index, dmin, dmax, 0, r->dist_d, nullptr, 1, p))) return rc;
     PhaseScope ps(r, 1);
-    ESB_CK(launch_bp(c, vol, voxel_type, r->dist_d, W, H, W, lambda, cf.oversampling, ray, ray + step, 1, r->stream),
-           "back projection");
+    ESB_CK(rec_bp(r, c, vol, voxel_type, r->dist_d, lambda, ray, ray + step, 1), "back projection");
   }
   return ESB_OK;
 }
@@ -642,14 +793,38 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
         if (active && !active[(size_t)p * np + index]) continue;
         KConst c = rec_const(r, pair_geoms[(size_t)p * np + index], sub_geoms[p], 1);
         PhaseScope ps(r, 1);
-        ESB_CK(launch_bp(c, boxes[p], ESB_VOXEL_F32, proj, W, H, W, 1.0f, cf.oversampling, 0.0f, 9999999999999.0f, 0,
-                         r->stream), "esb_subvolume_wbp");
+        ESB_CK(rec_bp(r, c, boxes[p], ESB_VOXEL_F32, proj, 1.0f, 0.0f, 9999999999999.0f, 0), "esb_subvolume_wbp");
       }
       continue;
     }
     float t_in, t_out;
     esb_defocus_distances(&r->geoms[index], full_vol, W, H, &t_in, &t_out);
     const float step = cf.ctf_slice_thickness_nm / cf.pixel_size_nm;
+    if (cf.variant == ESB_VARIANT_FAST) {
+      // Wiener-filtered image per slab of the whole tomogram, then one launch
+      // per particle that picks each quad's slab image by its depth
+      SlabTable T;
+      if ((rc = rec_slab_table(r, full_vol, index, T))) return rc;
+      if ((rc = rec_slab_capacity(r, T.count))) return rc;
+      static const int none[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int k = 0; k < T.count; ++k) {
+        float dmin, dmax;
+        esb_defocus_min_max(T.bound[k], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
+                            cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
+                            cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
+        if ((rc = rec_ctf_chain(r, const_cast<float*>(proj), 0, none, index, dmin, dmax, 0, r->slab_imgs + k * img,
+                                nullptr, 0, none)))
+          return rc;
+      }
+      for (int p = 0; p < n_particles; ++p) {
+        if (active && !active[(size_t)p * np + index]) continue;
+        KConst c = rec_const(r, pair_geoms[(size_t)p * np + index], sub_geoms[p], 1);
+        PhaseScope ps(r, 1);
+        ESB_CK(launch_bp_fast_slabs(c, boxes[p], ESB_VOXEL_F32, r->slab_imgs, img, T, W, H, W, 1.0f, cf.oversampling,
+                                    0.f, 0.f, 1, r->stream), "esb_subvolume_wbp");
+      }
+      continue;
+    }
     for (float ray = t_in; ray < t_out; ray += step) {
       float dmin, dmax;
       esb_defocus_min_max(ray, r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index], cf.add_tilt_angle,
@@ -662,8 +837,7 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
         if (active && !active[(size_t)p * np + index]) continue;
         KConst c = rec_const(r, pair_geoms[(size_t)p * np + index], sub_geoms[p], 1);
         PhaseScope ps(r, 1);
-        ESB_CK(launch_bp(c, boxes[p], ESB_VOXEL_F32, r->dist_d, W, H, W, 1.0f, cf.oversampling, ray, ray + step, 1,
-                         r->stream), "esb_subvolume_wbp");
+        ESB_CK(rec_bp(r, c, boxes[p], ESB_VOXEL_F32, r->dist_d, 1.0f, ray, ray + step, 1), "esb_subvolume_wbp");
       }
     }
   }

@@ -45,6 +45,16 @@ inline KConst to_kconst(const esb_constants& c) {
   return k;
 }
 
+// Defocus slabs of one projection (the reference's loop
+// for (ray = t_in; ray < t_out; ray += thickness), Reconstructor.cpp:515,
+// 935): slab k spans bound[k] <= t < bound[k+1] with the float recurrence
+// bound[k+1] = bound[k] + thickness. Slab images are k * stride apart.
+#define ESB_MAX_SLABS 256
+struct SlabTable {
+  int count;
+  float bound[ESB_MAX_SLABS + 1];
+};
+
 // Constants of kernel `ctf` (SetConstantValues(CTFKernel...), Kernels.cpp:1104-1131).
 struct CtfConst {
   float cs, lambda, ampC, phaseC, freqStep, pixelcount;

@@ -27,6 +27,7 @@ from . import _lib as L
 from ._lib import check, fptr, lib
 
 VOXEL_F32, VOXEL_F16, VOXEL_BF16 = L.VOXEL_F32, L.VOXEL_F16, L.VOXEL_BF16
+VARIANT_FAITHFUL, VARIANT_FAST = L.VARIANT_FAITHFUL, L.VARIANT_FAST
 PLT_NORMAL, PLT_RANDOM, PLT_RANDOM_START_ZERO_TILT = 0, 1, 2
 FM_RAMP, FM_EXACT, FM_CONTRAST2, FM_CONTRAST10, FM_CONTRAST30 = range(5)
 
@@ -160,18 +161,20 @@ def _img_args(img):
     return w, h, img.stride(-2) * 4
 
 
-def forward_project(c: L.Constants, vol, proj, dist, roi=None, stream=None) -> None:
-    """FPKernel: proj += line integrals, dist = mean chord (Kernels.cpp:46-88)."""
+def forward_project(c: L.Constants, vol, proj, dist, roi=None, stream=None, fast: bool = False) -> None:
+    """FPKernel: proj += line integrals, dist = mean chord (Kernels.cpp:46-88).
+    fast selects the closed-form cell-sum projector."""
     w, h, pitch = _img_args(proj)
     x0, y0, x1, y1 = roi if roi is not None else (0, 0, w, h)
-    check(lib.esb_fp(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(proj), fptr(dist), pitch, x0, y0, x1, y1,
+    check((lib.esb_fp_fast if fast else lib.esb_fp)(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(proj), fptr(dist), pitch, x0, y0, x1, y1,
                      _stream(stream)))
 
 
-def forward_project_slab(c: L.Constants, vol, proj, tmin: float, tmax: float, roi=None, stream=None) -> None:
+def forward_project_slab(c: L.Constants, vol, proj, tmin: float, tmax: float, roi=None, stream=None,
+                         fast: bool = False) -> None:
     w, h, pitch = _img_args(proj)
     x0, y0, x1, y1 = roi if roi is not None else (0, 0, w, h)
-    check(lib.esb_fp_slicer(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(proj), pitch, tmin, tmax, x0, y0,
+    check((lib.esb_fp_slicer_fast if fast else lib.esb_fp_slicer)(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(proj), pitch, tmin, tmax, x0, y0,
                             x1, y1, _stream(stream)))
 
 
@@ -196,10 +199,11 @@ def crop_border(img, cut_length, dim_length, points, stream=None) -> None:
 
 
 def back_project(c: L.Constants, vol, img, lam: float, oversampling: int = 1, dist_min: float = 0.0,
-                 dist_max: float = 9999999999999.0, linear: bool = False, stream=None) -> None:
-    """BPKernel: vol += lam * sum(img*chord)/sum(chord) (Kernels.cpp:327-379)."""
+                 dist_max: float = 9999999999999.0, linear: bool = False, stream=None, fast: bool = False) -> None:
+    """BPKernel: vol += lam * sum(img*chord)/sum(chord) (Kernels.cpp:327-379).
+    fast selects the per-voxel-shadow back-projector."""
     w, h, pitch = _img_args(img)
-    check(lib.esb_bp(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(img), pitch, lam, oversampling, dist_min,
+    check((lib.esb_bp_fast if fast else lib.esb_bp)(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(img), pitch, lam, oversampling, dist_min,
                      dist_max, int(linear), _stream(stream)))
 
 
@@ -299,6 +303,7 @@ class ReconConfig:
     switch_ctf_direction: bool = False
     volume_shift: tuple = (0.0, 0.0, 0.0)
     add_tilt_angle: float = 0.0
+    variant: int = L.VARIANT_FAITHFUL
 
     def c(self) -> L.ReconConfig:
         r = L.ReconConfig()
@@ -317,6 +322,7 @@ class ReconConfig:
         r.switch_ctf_direction = int(self.switch_ctf_direction)
         r.volume_shift[:] = list(self.volume_shift)
         r.add_tilt_angle = self.add_tilt_angle
+        r.variant = self.variant
         return r
 
 

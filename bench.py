@@ -221,7 +221,10 @@ def run_esb(args):
     params = dict(WL.CONFIGS[args.workload])
     wl = WL.build(args.workload, params, seed=rank)
     stream = torch.cuda.Stream()
-    rec = E.Reconstructor(wl.cfg, wl.pg, wl.tilt, wl.defocus, stream=stream)
+    import dataclasses
+
+    cfg = dataclasses.replace(wl.cfg, variant=E.VARIANT_FAST if args.variant == "fast" else E.VARIANT_FAITHFUL)
+    rec = E.Reconstructor(cfg, wl.pg, wl.tilt, wl.defocus, stream=stream)
     vol = torch.zeros(params["dims"][::-1], dtype=torch.float32, device=dev)
     sirt = params["sirt"]
 
@@ -314,7 +317,7 @@ def run_esb(args):
                 "config": {"workload": args.workload, "volume": list(params["dims"]),
                            "projections": params["n_proj"], "projection_size": [params["W"], params["H"]],
                            "oversampling": params["os"], "sirt_count": sirt, "ctf": params["ctf"],
-                           "ctf_slab_nm": 30.0, "voxel_storage": "f32",
+                           "ctf_slab_nm": 30.0, "voxel_storage": "f32", "kernels": args.variant,
                            "l2": "inputs larger than L2 (volume 1 GiB)", "parallelism": f"replicas x{ws}"},
                 "e2e": {"value": e2e_value, "unit": UNIT,
                         "h2d_bytes_per_step": int(wl.projections.numel() * 4),
@@ -343,6 +346,9 @@ def main():
     ap.add_argument("--impl", choices=["esb", "reference"], default="esb")
     ap.add_argument("--workload", default="c2_sart_ctf")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", choices=["fast", "faithful"], default="fast",
+                    help="fast: closed-form cell-sum projector and per-voxel-shadow back-projector; "
+                         "faithful: the reference's per-sample arithmetic")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

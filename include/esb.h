@@ -190,6 +190,22 @@ int esb_crop_border(int proj_x, int proj_y, size_t pitch, float* img, const floa
 int esb_bp(const esb_constants* c, void* vol, int voxel_type, int proj_x, int proj_y, const float* img, size_t pitch,
            float lambda, int oversampling, float dist_min, float dist_max, int linear_filter, void* stream);
 
+/* Reformulated ("fast") variants of the three entry points above, same
+ * arguments and results within rel-L2 1e-3 of the reference's arithmetic:
+ * esb_fp_fast / esb_fp_slicer_fast sum the trilinear interpolant over each
+ * crossed cell in closed form (the reference's sample positions, one cell
+ * load per ~5 samples); esb_bp_fast visits only each voxel's own shadow and
+ * computes chords in voxel-local coordinates. No counterpart in the
+ * reference beyond the kernels they reformulate. */
+int esb_fp_fast(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj,
+                float* dist, size_t pitch, int roi_x0, int roi_y0, int roi_x1, int roi_y1, void* stream);
+int esb_fp_slicer_fast(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj,
+                       size_t pitch, float tmin, float tmax, int roi_x0, int roi_y0, int roi_x1, int roi_y1,
+                       void* stream);
+int esb_bp_fast(const esb_constants* c, void* vol, int voxel_type, int proj_x, int proj_y, const float* img,
+                size_t pitch, float lambda, int oversampling, float dist_min, float dist_max, int linear_filter,
+                void* stream);
+
 /* CopyToSquareKernel::operator() (Kernels.cpp:808-850) -> `makeSquare`
  * (CopyToSquare.cu:38-92); out is dense maxsize x maxsize. */
 int esb_make_square(int proj_x, int proj_y, size_t pitch, const float* in, int maxsize, float* out, int border_x,
@@ -251,7 +267,11 @@ typedef struct esb_recon_config {
   int switch_ctf_direction;       /* SwitchCTFDirectionForIMOD */
   float volume_shift[3];          /* VolumeShift */
   float add_tilt_angle;           /* AddTiltAngle */
+  int variant;                    /* ESB_VARIANT_FAITHFUL or ESB_VARIANT_FAST kernels */
 } esb_recon_config;
+
+#define ESB_VARIANT_FAITHFUL 0
+#define ESB_VARIANT_FAST 1
 
 typedef struct esb_reconstructor esb_reconstructor;
 

@@ -1,0 +1,247 @@
+"""Parity of the reformulated ("fast") kernels.
+
+Forward projection: the closed-form cell sums use the reference's sample
+positions without the reference's per-sample position rounding (~1e-3 voxel
+jitter). Against the FP32 and FP64 oracles: rel-L2 <= 1e-4.
+
+Back-projection: the fast kernel computes exact chords. The reference's FP32
+chords carry rounding noise from ray origins 1e5 units away. On random
+images a single update differs from the exact (FP64) update by 0.3-1%
+rel-L2, and the FP32 oracle reproduces that noise. The fast kernel is held to
+the FP64 oracle per update (rel-L2 <= 1e-5) and to both oracles on SART
+volumes, the north-star measure (FP32: <= 1e-3; FP64: <= 2e-4).
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import cuda, host, rel_l2, small_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    return small_case(shift=1.5, psi=0.3)
+
+
+def _orc(case, i, for_bp=False, aniso=None):
+    from oracle import geometry as G
+
+    m, mi = (None, None) if aniso is None else aniso
+    return G.orc_geom(case["og"][i], case["vo"], m, mi, for_bp=for_bp)
+
+
+@pytest.mark.parametrize("voxel", ["f32", "bf16"])
+def test_fast_forward_projection(case, voxel):
+    import torch
+
+    import artiatomi_b200 as E
+    from oracle import driver as D, lib as OL
+
+    W, H = case["W"], case["H"]
+    vol32 = case["vol"]
+    if voxel == "f32":
+        vol_d, vol_o, code = cuda(vol32), vol32, 0
+    else:
+        vol_d = cuda(vol32).to(torch.bfloat16)
+        vol_o, code = np.zeros(vol32.shape, np.uint16), 2
+        OL.olib.orc_float_to_bf16(OL.addr(vol32), OL.addr(vol_o), vol32.size)
+    m = E.mag_aniso_matrix(1.02, 30.0, W, H)
+    mi = E.mag_aniso_matrix(1.0 / 1.02, 30.0, W, H)
+    for aniso in (None, (m, mi)):
+        for i in range(len(case["tilt"])):
+            c = E.set_constant_values(case["pg"][i], case["vg"], *(aniso or (None, None)))
+            proj = torch.zeros((H, W), device="cuda")
+            dist = torch.zeros((H, W), device="cuda")
+            E.forward_project(c, vol_d, proj, dist, fast=True)
+            for prec in (0, 1):
+                po = np.zeros((H, W), np.float32)
+                do = np.zeros((H, W), np.float32)
+                D.fp_march(_orc(case, i, aniso=aniso), vol_o, code, W, H, po, do, precision=prec)
+                e = rel_l2(host(proj), po)
+                assert e <= 2e-4, (i, prec, e)
+                # ray lengths: the FP32 values are the reference's (t ~ 1e4 rounds
+                # to ~1e-3); FP64 lengths differ from them by that rounding
+                e = rel_l2(host(dist), do)
+                assert e <= (1e-6 if prec == 0 else 1e-4), (i, prec, e)
+
+
+def test_fast_slicer(case):
+    import torch
+
+    import artiatomi_b200 as E
+    from oracle import driver as D
+    from oracle import geometry as G
+
+    W, H = case["W"], case["H"]
+    vol_d = cuda(case["vol"])
+    for i in range(len(case["tilt"])):
+        t0, t1 = G.defocus_distances(case["og"][i], case["vo"])
+        for a, b in ((t0, t0 + 7.5), (0.5 * (t0 + t1) - 3.0, 0.5 * (t0 + t1) + 9.0), (t1 - 4.0, t1 + 20.0)):
+            c = E.set_constant_values(case["pg"][i], case["vg"])
+            proj = torch.zeros((H, W), device="cuda")
+            E.forward_project_slab(c, vol_d, proj, a, b, fast=True)
+            po = np.zeros((H, W), np.float32)
+            D.fp_slicer(_orc(case, i), case["vol"], 0, W, H, po, a, b)
+            e = rel_l2(host(proj), po)
+            assert e <= 1e-4, (i, a, b, e)
+
+
+@pytest.mark.parametrize("os_,linear,slab", [(1, False, False), (2, False, False), (2, True, True), (3, True, False)])
+def test_fast_back_projection_exact_chords(case, os_, linear, slab):
+    import artiatomi_b200 as E
+    from oracle import driver as D
+    from oracle import geometry as G
+
+    W, H = case["W"], case["H"]
+    rng = np.random.default_rng(17)
+    vol0 = rng.normal(size=case["vol"].shape).astype(np.float32)
+    for i in range(len(case["tilt"])):
+        img = rng.normal(size=(H, W)).astype(np.float32)
+        dmin, dmax = 0.0, 9999999999999.0
+        if slab:
+            t0, t1 = G.defocus_distances(case["og"][i], case["vo"])
+            dmin, dmax = 0.5 * (t0 + t1) - 8.0, 0.5 * (t0 + t1) + 8.0
+        v_d = cuda(vol0)
+        E.back_project(E.set_constant_values(case["pg"][i], case["vg"], for_bp=True), v_d, cuda(img), 0.37, os_, dmin,
+                       dmax, linear, fast=True)
+        vo = vol0.copy()
+        D.bp(_orc(case, i, for_bp=True), vo, 0, img, 0.37, os_, dmin, dmax, int(linear), precision=1)
+        e = rel_l2(host(v_d) - vol0, vo - vol0)
+        # the sub-pixel grid is the reference's float recurrence from the
+        # quad's macro-cell corner (exact lattice for power-of-two OS only)
+        assert e <= 1e-5, (i, e)
+
+
+@pytest.mark.parametrize("sirt,os_", [(1, 1), (3, 2)])
+def test_fast_sart_volume(sirt, os_):
+    import artiatomi_b200 as E
+    from oracle.driver import OracleReconstructor
+    from tests.test_parity_recon import _projections
+
+    case = small_case(n_proj=9, shift=1.0, psi=0.2)
+    W, H = case["W"], case["H"]
+    projs = _projections(case)
+    il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, case["tilt"])
+    cfgd = dict(lambda_=0.5, oversampling=os_, cut_length=(1.0, 1.0), dim_length=(3.0, 3.0),
+                crop=(1.0, 2.0, 1.0, 2.0), crop_dim=(3.0, 3.0, 3.0, 3.0))
+    rec = E.Reconstructor(E.ReconConfig(W, H, len(case["tilt"]), variant=E.VARIANT_FAST, **cfgd), case["pg"],
+                          case["tilt"])
+    vol_d = cuda(np.zeros(case["vol"].shape, np.float32))
+    rec.sart(case["vg"], vol_d, cuda(projs), il, iterations=2, sirt_count=sirt)
+    got = host(vol_d)
+    for prec, tol in ((0, 1e-3), (1, 2e-4)):
+        orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], precision=prec)
+        vo = np.zeros(case["vol"].shape, np.float32)
+        orc.sart(case["vo"], vo, 0, projs, il, 2, sirt)
+        e = rel_l2(got, vo)
+        assert e <= tol, (prec, e)
+
+
+def _defocus(n, seed):
+    rng = np.random.default_rng(seed)
+    d = np.stack([rng.uniform(2900, 3100, n), rng.uniform(3100, 3200, n), rng.uniform(0, 180, n)], 1)
+    return d.astype(np.float32).ravel()
+
+
+def test_fast_ctf_forward_and_back_projection():
+    """Fused multi-slab slicer + per-slab CTF, and the fused slab back-projection."""
+    import artiatomi_b200 as E
+    from oracle.driver import OracleReconstructor
+    from tests.test_parity_recon import _ctf_cfg
+
+    case = small_case(dims=(64, 64, 24), n_proj=5, shift=1.0)
+    W, H = case["W"], case["H"]
+    n = len(case["tilt"])
+    defocus = _defocus(n, 5)
+    cfgd = _ctf_cfg(W)
+    rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **cfgd), case["pg"], case["tilt"], defocus)
+    vol_d = cuda(case["vol"])
+    proj_v, dist_v, _ = rec.views()
+    for prec in (0, 1):
+        orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], defocus, precision=prec)
+        for i in range(n):
+            rec.reset_projections()
+            rec.forward_projection(case["vg"], vol_d, i, False)
+            orc.reset()
+            orc.forward_projection(case["vo"], case["vol"], 0, i, False)
+            e = rel_l2(host(proj_v), orc.proj)
+            assert e <= 1e-4, (prec, i, e)
+    rng = np.random.default_rng(6)
+    vol_b = cuda(np.zeros(case["vol"].shape, np.float32))
+    vo = np.zeros(case["vol"].shape, np.float32)
+    orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], defocus, precision=1)
+    for i in range(n):
+        res = rng.normal(size=(H, W)).astype(np.float32)
+        proj_v.copy_(cuda(res))
+        rec.back_projection(case["vg"], vol_b, i, 2.0)
+        orc.back_projection(case["vo"], vo, 0, i, 2.0, img=res.copy())
+    e = rel_l2(host(vol_b), vo)
+    assert e <= 1e-4, e
+
+
+def test_fast_sart_ctf():
+    import artiatomi_b200 as E
+    from oracle.driver import OracleReconstructor
+    from tests.test_parity_recon import _ctf_cfg, _projections
+
+    case = small_case(dims=(64, 64, 24), n_proj=5, shift=0.5)
+    W, H = case["W"], case["H"]
+    n = len(case["tilt"])
+    defocus = _defocus(n, 15)
+    projs = _projections(case)
+    il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, case["tilt"])
+    cfgd = dict(_ctf_cfg(W), lambda_=0.5, oversampling=2)
+    rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **cfgd), case["pg"], case["tilt"], defocus)
+    vol_d = cuda(np.zeros(case["vol"].shape, np.float32))
+    rec.sart(case["vg"], vol_d, cuda(projs), il, iterations=2, sirt_count=2)
+    got = host(vol_d)
+    for prec, tol in ((0, 1e-3), (1, 2e-4)):
+        orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], defocus, precision=prec)
+        vo = np.zeros(case["vol"].shape, np.float32)
+        orc.sart(case["vo"], vo, 0, projs, il, 2, 2)
+        e = rel_l2(got, vo)
+        assert e <= tol, (prec, e)
+
+
+@pytest.mark.parametrize("ctf", [False, True])
+def test_fast_subvolume_wbp(ctf):
+    import artiatomi_b200 as E
+    from artiatomi_b200 import _lib as L
+    from oracle import geometry as G
+    from oracle.driver import OracleReconstructor
+
+    W = H = 96
+    n = 7
+    tilt = np.linspace(-60, 60, n).astype(np.float32)
+    rng = np.random.default_rng(31)
+    projs = rng.normal(size=(n, H, W)).astype(np.float32)
+    full, fo = E.volume_geometry((96, 96, 40)), G.volume_geometry((96, 96, 40))
+    sizes = [16, 24, 16, 32]
+    pos = rng.uniform(20, 76, size=(len(sizes), 3))
+    pos[:, 2] = rng.uniform(10, 30, len(sizes))
+    shifts = rng.uniform(-1.5, 1.5, size=(len(sizes), n, 2)).astype(np.float32)
+    sub = [E.subvolume_geometry(s, 1.0, full, p) for s, p in zip(sizes, pos)]
+    subo = [G.subvolume_geometry(s, 1.0, fo, p) for s, p in zip(sizes, pos)]
+    pair = (L.ProjGeom * (len(sizes) * n))()
+    pair_o = []
+    for p in range(len(sizes)):
+        g = E.projection_geometry(E.Markers(tilt), W, H, extra_shift=shifts[p])
+        for i in range(n):
+            pair[p * n + i] = g[i]
+        pair_o.append(G.projection_geometry(tilt, width=W, height=H, extra_shift=shifts[p]))
+    defocus = np.stack([np.full(n, 3000.0), np.full(n, 3100.0), np.full(n, 20.0)], 1).astype(np.float32).ravel()
+    cfgd = dict(oversampling=2, ctf_mode=ctf, pixel_size_nm=0.27, ctf_slice_thickness_nm=4.0,
+                ctf_beta_fac=(10.0, 0.0, 0.008, 0.0))
+    pg = E.projection_geometry(E.Markers(tilt), W, H)
+    rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **cfgd), pg, tilt, defocus if ctf else None)
+    boxes = [cuda(np.zeros((s, s, s), np.float32)) for s in sizes]
+    il = np.arange(n, dtype=np.int32)
+    rec.subvolume_wbp(full, sub, pair, boxes, cuda(projs), il)
+    orc = OracleReconstructor(cfgd, W, H, G.projection_geometry(tilt, width=W, height=H), tilt,
+                              defocus if ctf else None, precision=1)
+    bo = [np.zeros((s, s, s), np.float32) for s in sizes]
+    orc.subvolume_wbp(fo, subo, pair_o, bo, projs, il)
+    for b, o in zip(boxes, bo):
+        e = rel_l2(host(b), o)
+        assert e <= 1e-4, e
