@@ -27,7 +27,7 @@ cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img,
                            float lambda, int os, float distMin, float distMax, int linear, cudaStream_t st);
 cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
                                  const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
-                                 float distMin, float distMax, int linear, cudaStream_t st);
+                                 float distMin, float distMax, int linear, cudaStream_t st, int transposed);
 cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float* imgs, size_t img_stride,
                                 size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1, cudaStream_t st);
 cudaError_t launch_compare(int pw, int ph, size_t pitchE, const float* real, float* virt, const float* dist,
@@ -40,7 +40,8 @@ cudaError_t launch_crop_to_square(int pw, int ph, size_t pitchE, float* img, int
                                   const int* p, int maxsize, float* sq, int bx, int by, cudaStream_t st);
 cudaError_t launch_square_to_image(const float* sq, int maxsize, size_t shift, float inv_norm, int pw, int ph,
                                    size_t pitchE, float* out, float* accum, int apply_crop, float2 cut, float2 dim,
-                                   const int* p, cudaStream_t st);
+                                   const int* p, cudaStream_t st, int transpose_out);
+cudaError_t launch_transpose(const float* in, int w, int h, size_t pitchE, float* out, cudaStream_t st);
 CtfConst make_ctf_const(int n, float cs_mm, float voltage_kv, float amp_contrast, float pixel_size_nm);
 cudaError_t launch_ctf(float* spec, int n, const CtfConst& k, float d0_nm, float d1_nm, float angle_deg, int applyForFP,
                        int phaseFlip, float wiener, float4 beta, cudaStream_t st);
@@ -523,7 +524,8 @@ static KConst rec_const(esb_reconstructor* r, const esb_proj_geom& g, const esb_
 // N x N square, R2C, CTF (FP or Wiener BP), C2R, scale 1/N^2, crop, and write
 // to `out` and/or accumulate into `accum` (Reconstructor.cpp:559-583, 952-965).
 static int rec_ctf_chain(esb_reconstructor* r, float* img, int crop_in, const int* p_in, int index, float dmin,
-                         float dmax, int for_fp, float* out, float* accum, int crop_out, const int* p_out) {
+                         float dmax, int for_fp, float* out, float* accum, int crop_out, const int* p_out,
+                         int transpose_out = 0) {
   const esb_recon_config& cf = r->cfg;
   const int W = cf.proj_x, H = cf.proj_y, N = r->N;
   PhaseScope ps(r, 2);
@@ -537,7 +539,7 @@ static int rec_ctf_chain(esb_reconstructor* r, float* img, int crop_in, const in
                     cf.wiener_noise_level, beta, r->stream), "ctf chain");
   ESB_FFT(cufftExecC2R(r->c2r, (cufftComplex*)r->fft_d, (cufftReal*)r->square_d), "ctf chain C2R");
   ESB_CK(launch_square_to_image(r->square_d, N, r->squareShift, 1.0f / ((float)N * (float)N), W, H, W, out, accum,
-                                crop_out, cut, dim, p_out, r->stream), "ctf chain");
+                                crop_out, cut, dim, p_out, r->stream, transpose_out), "ctf chain");
   return ESB_OK;
 }
 
@@ -679,6 +681,20 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
       ESB_CK(launch_crop_border(W, H, W, img, make_float2(cf.cut_length[0], cf.cut_length[1]),
                                 make_float2(cf.dim_length[0], cf.dim_length[1]), p, r->stream), "back projection");
     }
+    if (cf.variant == ESB_VARIANT_FAST) {
+      int rc2;
+      if ((rc2 = rec_slab_capacity(r, 1))) return rc2;
+      {
+        PhaseScope ps(r, 3);
+        ESB_CK(launch_transpose(img, W, H, W, r->slab_imgs, r->stream), "back projection");
+      }
+      SlabTable none;
+      none.count = 0;
+      PhaseScope ps(r, 1);
+      ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, 0, none, W, H, W, lambda, cf.oversampling, 0.0f,
+                                  9999999999999.0f, 0, r->stream, 1), "back projection");
+      return ESB_OK;
+    }
     PhaseScope ps(r, 1);
     ESB_CK(rec_bp(r, c, vol, voxel_type, img, lambda, 0.0f, 9999999999999.0f, 0), "back projection");
     return ESB_OK;
@@ -700,11 +716,11 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
                           cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
                           cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
       // cropBorder(proj_d) is re-applied to the residual on every slab (:954)
-      if ((rc = rec_ctf_chain(r, img, 1, p, index, dmin, dmax, 0, r->slab_imgs + k * npx, nullptr, 1, p))) return rc;
+      if ((rc = rec_ctf_chain(r, img, 1, p, index, dmin, dmax, 0, r->slab_imgs + k * npx, nullptr, 1, p, 1))) return rc;
     }
     PhaseScope ps(r, 1);
     ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, npx, T, W, H, W, lambda, cf.oversampling, 0.f, 0.f,
-                                1, r->stream), "back projection");
+                                1, r->stream, 1), "back projection");
     return ESB_OK;
   }
   for (float ray = t_in; ray < t_out; ray += step) {
@@ -788,6 +804,20 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
     const int index = index_list[ii];
     if (index < 0 || index >= np) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_subvolume_wbp: index out of range");
     const float* proj = projections + (size_t)index * img;
+    if (!cf.ctf_mode && cf.variant == ESB_VARIANT_FAST) {
+      if ((rc = rec_slab_capacity(r, 1))) return rc;
+      ESB_CK(launch_transpose(proj, W, H, W, r->slab_imgs, r->stream), "esb_subvolume_wbp");
+      SlabTable none;
+      none.count = 0;
+      for (int p = 0; p < n_particles; ++p) {
+        if (active && !active[(size_t)p * np + index]) continue;
+        KConst c = rec_const(r, pair_geoms[(size_t)p * np + index], sub_geoms[p], 1);
+        PhaseScope ps(r, 1);
+        ESB_CK(launch_bp_fast_slabs(c, boxes[p], ESB_VOXEL_F32, r->slab_imgs, 0, none, W, H, W, 1.0f, cf.oversampling,
+                                    0.0f, 9999999999999.0f, 0, r->stream, 1), "esb_subvolume_wbp");
+      }
+      continue;
+    }
     if (!cf.ctf_mode) {
       for (int p = 0; p < n_particles; ++p) {
         if (active && !active[(size_t)p * np + index]) continue;
@@ -813,7 +843,7 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
                             cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
                             cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
         if ((rc = rec_ctf_chain(r, const_cast<float*>(proj), 0, none, index, dmin, dmax, 0, r->slab_imgs + k * img,
-                                nullptr, 0, none)))
+                                nullptr, 0, none, 1)))
           return rc;
       }
       for (int p = 0; p < n_particles; ++p) {
@@ -821,7 +851,7 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
         KConst c = rec_const(r, pair_geoms[(size_t)p * np + index], sub_geoms[p], 1);
         PhaseScope ps(r, 1);
         ESB_CK(launch_bp_fast_slabs(c, boxes[p], ESB_VOXEL_F32, r->slab_imgs, img, T, W, H, W, 1.0f, cf.oversampling,
-                                    0.f, 0.f, 1, r->stream), "esb_subvolume_wbp");
+                                    0.f, 0.f, 1, r->stream, 1), "esb_subvolume_wbp");
       }
       continue;
     }

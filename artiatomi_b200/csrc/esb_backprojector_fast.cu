@@ -29,19 +29,28 @@ namespace esb {
 
 namespace {
 
+// Image texel (ix, iy): row-major [y][x] with pitch, or transposed [x][y]
+// (the reconstructor's layout: threads of a warp walk the volume's x axis,
+// which maps to the detector's y axis, so a transposed image keeps their
+// reads contiguous).
+__device__ __forceinline__ float texel(const float* __restrict__ img, int h, size_t pitchE, bool transposed, int ix,
+                                       int iy) {
+  return __ldg(img + (transposed ? (size_t)ix * h + iy : (size_t)iy * pitchE + ix));
+}
+
 __device__ __forceinline__ float sample_image(const float* __restrict__ img, int w, int h, size_t pitchE, float x,
-                                              float y, bool linear) {
+                                              float y, bool linear, bool transposed) {
   if (!linear) {
     int ix = clamp_texel(floorf(x), w), iy = clamp_texel(floorf(y), h);
-    return __ldg(img + (size_t)iy * pitchE + ix);
+    return texel(img, h, pitchE, transposed, ix, iy);
   }
   float xb = x - 0.5f, yb = y - 0.5f;
   float fx = floorf(xb), fy = floorf(yb);
   float a = xb - fx, b = yb - fy;
   int x0 = clamp_texel(fx, w), x1 = clamp_texel(fx + 1.0f, w);
   int y0 = clamp_texel(fy, h), y1 = clamp_texel(fy + 1.0f, h);
-  float t00 = __ldg(img + (size_t)y0 * pitchE + x0), t10 = __ldg(img + (size_t)y0 * pitchE + x1);
-  float t01 = __ldg(img + (size_t)y1 * pitchE + x0), t11 = __ldg(img + (size_t)y1 * pitchE + x1);
+  float t00 = texel(img, h, pitchE, transposed, x0, y0), t10 = texel(img, h, pitchE, transposed, x1, y0);
+  float t01 = texel(img, h, pitchE, transposed, x0, y1), t11 = texel(img, h, pitchE, transposed, x1, y1);
   return (1.0f - b) * ((1.0f - a) * t00 + a * t10) + b * ((1.0f - a) * t01 + a * t11);
 }
 
@@ -133,7 +142,7 @@ template <int VT>
 __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __restrict__ vol,
                                                  const float* __restrict__ imgs, size_t img_stride, SlabTable slabs,
                                                  int pw, int ph, size_t pitchE, float lambda, int os, float inv,
-                                                 float distMin, float distMax, int linear) {
+                                                 float distMin, float distMax, int linear, int transposed) {
   const int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int z = (int)blockIdx.z;
@@ -174,7 +183,7 @@ __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __res
         if (L > 0.0f) {
           const float xA = k.anisoInv[0] * px + k.anisoInv[1] * py + k.anisoInv[2];
           const float yA = k.anisoInv[3] * px + k.anisoInv[4] * py + k.anisoInv[5];
-          a += sample_image(img, pw, ph, pitchE, xA, yA, linear != 0) * L;
+          a += sample_image(img, pw, ph, pitchE, xA, yA, linear != 0, transposed != 0) * L;
           da += L;
         }
       }
@@ -219,16 +228,16 @@ BpGeom make_geom(const KConst& k, int os) {
 
 cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
                                  const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
-                                 float distMin, float distMax, int linear, cudaStream_t st) {
+                                 float distMin, float distMax, int linear, cudaStream_t st, int transposed) {
   const int nq = k.dimXQuarter, ny = (int)k.dim.y, nz = (int)k.dim.z;
   if (nq <= 0 || ny <= 0 || nz <= 0) return cudaSuccess;
   const BpGeom g = make_geom(k, os);
   const float inv = 1.0f / (float)os;
   dim3 blk(32, 4, 1), grd((nq + 31) / 32, (ny + 3) / 4, nz);
   switch (vt) {
-    case ESB_VOXEL_F32: k_bp_fast<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); break;
-    case ESB_VOXEL_F16: k_bp_fast<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); break;
-    default: k_bp_fast<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); break;
+    case ESB_VOXEL_F32: k_bp_fast<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); break;
+    case ESB_VOXEL_F16: k_bp_fast<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); break;
+    default: k_bp_fast<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); break;
   }
   return cudaGetLastError();
 }
@@ -237,7 +246,7 @@ cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img,
                            float lambda, int os, float distMin, float distMax, int linear, cudaStream_t st) {
   SlabTable none;
   none.count = 0;
-  return launch_bp_fast_slabs(k, vol, vt, img, 0, none, pw, ph, pitchE, lambda, os, distMin, distMax, linear, st);
+  return launch_bp_fast_slabs(k, vol, vt, img, 0, none, pw, ph, pitchE, lambda, os, distMin, distMax, linear, st, 0);
 }
 
 }  // namespace esb

@@ -133,15 +133,31 @@ __global__ void k_crop_to_square(int pw, int ph, size_t pitchE, float* __restric
 // accumulation into proj (Reconstructor.cpp:578-583, 962-965).
 __global__ void k_square_to_image(const float* __restrict__ sq, int maxsize, size_t shift, float inv_norm, int pw,
                                   int ph, size_t pitchE, float* __restrict__ out, float* __restrict__ accum,
-                                  int apply_crop, float2 cut, float2 dim, int2 p1, int2 p2, int2 p3, int2 p4) {
+                                  int apply_crop, float2 cut, float2 dim, int2 p1, int2 p2, int2 p3, int2 p4,
+                                  int transpose_out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= pw || y >= ph) return;
   float v = sq[shift + (size_t)y * maxsize + x] * inv_norm;
   if (apply_crop) v = crop_factor(pw, ph, x, y, cut, dim, p1, p2, p3, p4) * v;
   const size_t i = (size_t)y * pitchE + x;
-  if (out) out[i] = v;
+  if (out) out[transpose_out ? (size_t)x * ph + y : i] = v;
   if (accum) accum[i] += v;
+}
+
+// out[x][y] = in[y][x] for a W x H image (32x32 tiles through shared memory).
+__global__ void k_transpose(const float* __restrict__ in, int w, int h, size_t pitchE, float* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int x = bx + threadIdx.x, y = by + j;
+    if (x < w && y < h) tile[j][threadIdx.x] = in[(size_t)y * pitchE + x];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int y = by + threadIdx.x, x = bx + j;
+    if (x < w && y < h) out[(size_t)x * h + y] = tile[threadIdx.x][j];
+  }
 }
 
 // Kernel `ctf` (ctf.cu:82-240).
@@ -319,11 +335,17 @@ cudaError_t launch_crop_to_square(int pw, int ph, size_t pitchE, float* img, int
 
 cudaError_t launch_square_to_image(const float* sq, int maxsize, size_t shift, float inv_norm, int pw, int ph,
                                    size_t pitchE, float* out, float* accum, int apply_crop, float2 cut, float2 dim,
-                                   const int* p, cudaStream_t st) {
+                                   const int* p, cudaStream_t st, int transpose_out) {
   dim3 b(32, 8);
   k_square_to_image<<<grid2(pw, ph, b), b, 0, st>>>(sq, maxsize, shift, inv_norm, pw, ph, pitchE, out, accum,
                                                     apply_crop, cut, dim, make_int2(p[0], p[1]), make_int2(p[2], p[3]),
-                                                    make_int2(p[4], p[5]), make_int2(p[6], p[7]));
+                                                    make_int2(p[4], p[5]), make_int2(p[6], p[7]), transpose_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose(const float* in, int w, int h, size_t pitchE, float* out, cudaStream_t st) {
+  dim3 b(32, 8), g((w + 31) / 32, (h + 31) / 32);
+  k_transpose<<<g, b, 0, st>>>(in, w, h, pitchE, out);
   return cudaGetLastError();
 }
 

@@ -27,6 +27,10 @@ CONFIGS = {
     # 100 nm, 30 nm slabs, oversampling 2, 4 projections per subset.
     "c2_sart_ctf": dict(dims=(1024, 1024, 256), W=1024, H=1024, n_proj=61, n_ell=5000, n_beads=300, ctf=True, os=2,
                         sirt=4, lam=0.5, iterations=2, shift=2.0, psi=0.3, snr=0.1),
+    # The same geometry with a 64-voxel-thick volume (256 MiB, still larger
+    # than L2): the case on which kernels are profiled with ncu.
+    "c2_sart_ctf_z64": dict(dims=(1024, 1024, 64), W=1024, H=1024, n_proj=61, n_ell=1250, n_beads=75, ctf=True, os=2,
+                            sirt=4, lam=0.5, iterations=2, shift=2.0, psi=0.3, snr=0.1),
 }
 
 

@@ -59,7 +59,9 @@ def test_fast_forward_projection(case, voxel):
                 do = np.zeros((H, W), np.float32)
                 D.fp_march(_orc(case, i, aniso=aniso), vol_o, code, W, H, po, do, precision=prec)
                 e = rel_l2(host(proj), po)
-                assert e <= 2e-4, (i, prec, e)
+                # FP32: the reference's float ray positions (start point s + t*n
+                # at |t| ~ 1e4) are shared; FP64 positions differ by ~1e-3 voxel
+                assert e <= (1e-4 if prec == 0 else 5e-4), (i, prec, e)
                 # ray lengths: the FP32 values are the reference's (t ~ 1e4 rounds
                 # to ~1e-3); FP64 lengths differ from them by that rounding
                 e = rel_l2(host(dist), do)
