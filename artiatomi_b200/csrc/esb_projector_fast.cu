@@ -185,6 +185,79 @@ __device__ float cell_sum(const Cell<VT>& C, float qx, float qy, float qz, float
   return acc;
 }
 
+// cell_sum for a ray whose y coordinate stays in one interpolation cell with
+// a constant weight b (single-axis tilt about y: n.y is 0 or ~1e-10): the
+// trilinear interpolant is a bilinear one in (x, z) of the y-interpolated
+// corners, walked with a 2-D DDA.
+template <int VT>
+__device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float qz, float dqx, float dqz, int j0,
+                             int J) {
+  if (j0 >= J) return 0.0f;
+  const float px = qx + (float)j0 * dqx, pz = qz + (float)j0 * dqz;
+  const float fx = floorf(px), fz = floorf(pz);
+  int ix = (int)fx, iz = (int)fz;
+  const float inf = FLT_MAX;
+  const float isx = dqx != 0.f ? 1.0f / fabsf(dqx) : inf;
+  const float isz = dqz != 0.f ? 1.0f / fabsf(dqz) : inf;
+  float nxs = dqx > 0.f ? (fx + 1.f - px) * isx : (dqx < 0.f ? (px - fx) * isx : inf);
+  float nzs = dqz > 0.f ? (fz + 1.f - pz) * isz : (dqz < 0.f ? (pz - fz) * isz : inf);
+  const int stx = dqx > 0.f ? 1 : -1, stz = dqz > 0.f ? 1 : -1;
+  const float ib = 1.0f - b;
+  const long y0 = (long)(iy < 0 ? 0 : (iy > C.ny - 1 ? C.ny - 1 : iy)) * C.sy;
+  const long y1 = (long)(iy + 1 < 0 ? 0 : (iy + 1 > C.ny - 1 ? C.ny - 1 : iy + 1)) * C.sy;
+  auto ey = [&](int x, int z) {
+    x = x < 0 ? 0 : (x > C.nx - 1 ? C.nx - 1 : x);
+    z = z < 0 ? 0 : (z > C.nz - 1 ? C.nz - 1 : z);
+    const long o = (long)z * C.sz + x;
+    return ib * Voxel<VT>::load(C.vol, o + y0) + b * Voxel<VT>::load(C.vol, o + y1);
+  };
+  float e00 = ey(ix, iz), e10 = ey(ix + 1, iz), e01 = ey(ix, iz + 1), e11 = ey(ix + 1, iz + 1);
+  const int M_total = J - j0;
+  int m0 = 0;
+  float acc = 0.0f;
+#pragma unroll 1
+  for (int guard = 0; guard < 1 << 20; ++guard) {
+    const float sexit = fminf(nxs, nzs);
+    int m1 = (sexit >= (float)M_total) ? M_total : (int)ceilf(sexit);
+    if (m1 > M_total) m1 = M_total;
+    if (m1 > m0) {
+      const float a0 = (qx + (float)(j0 + m0) * dqx) - (float)ix;
+      const float c0 = (qz + (float)(j0 + m0) * dqz) - (float)iz;
+      const float M = (float)(m1 - m0);
+      const float S1 = 0.5f * M * (M - 1.f);
+      const float S2 = S1 * (2.f * M - 1.f) * (1.f / 3.f);
+      const float k1 = e10 - e00, k3 = e01 - e00, k5 = e11 - e10 - e01 + e00;
+      const float sa = M * a0 + S1 * dqx, sc = M * c0 + S1 * dqz;
+      const float sac = M * a0 * c0 + S1 * (a0 * dqz + c0 * dqx) + S2 * dqx * dqz;
+      acc += e00 * M + k1 * sa + k3 * sc + k5 * sac;
+      m0 = m1;
+    }
+    if (m0 >= M_total) break;
+    if (nxs <= nzs) {
+      ix += stx;
+      nxs = stx > 0 ? ((float)(ix + 1) - px) * isx : (px - (float)ix) * isx;
+      if (stx > 0) {
+        e00 = e10; e01 = e11;
+        e10 = ey(ix + 1, iz); e11 = ey(ix + 1, iz + 1);
+      } else {
+        e10 = e00; e11 = e01;
+        e00 = ey(ix, iz); e01 = ey(ix, iz + 1);
+      }
+    } else {
+      iz += stz;
+      nzs = stz > 0 ? ((float)(iz + 1) - pz) * isz : (pz - (float)iz) * isz;
+      if (stz > 0) {
+        e00 = e01; e10 = e11;
+        e01 = ey(ix, iz + 1); e11 = ey(ix + 1, iz + 1);
+      } else {
+        e01 = e00; e11 = e10;
+        e00 = ey(ix, iz); e10 = ey(ix + 1, iz);
+      }
+    }
+  }
+  return acc;
+}
+
 // Ray start and box entry/exit: the reference's expressions, operation by
 // operation without contraction, so t_in/t_out (|t| ~ 1e4) and hence the
 // sample positions and ray lengths equal the reference's FP32 values.
@@ -257,12 +330,18 @@ __device__ float ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0,
     sum += trilinear<VT>(C, q.x, q.y, q.z);
     j0 = 1;
   }
+  // y stays in one cell and moves by < 1e-5 voxel over the ray: bilinear x-z walk
+  const float ylast = q0.y + (float)(J - 1) * dqy;
+  if (fabsf(dqy) * (float)J < 1e-5f && floorf(q0.y) == floorf(ylast)) {
+    const float fy = floorf(q0.y);
+    return sum + cell_sum_xz<VT>(C, q0.x, q0.y - fy, (int)fy, q0.z, dqx, dqz, j0, J);
+  }
   return sum + cell_sum<VT>(C, q0.x, q0.y, q0.z, dqx, dqy, dqz, j0, J);
 }
 
 // mode 0: march (proj += sum/4, dist = mean chord); mode 1: slicer (proj += sum/4 within [tmin, tmax])
 template <int VT, int MODE>
-__global__ void __launch_bounds__(256) k_project_fast(KConst c, const void* __restrict__ vol, float* __restrict__ proj,
+__global__ void __launch_bounds__(256, 3) k_project_fast(KConst c, const void* __restrict__ vol, float* __restrict__ proj,
                                                       float* __restrict__ dist, size_t pitchE, float tminDef,
                                                       float tmaxDef, int x0, int y0, int x1, int y1) {
   // lanes: 4 sub-rays of a pixel adjacent; a warp spans 8 detector rows (v)
@@ -308,7 +387,7 @@ __global__ void __launch_bounds__(256) k_project_fast(KConst c, const void* __re
 // walk the union of their slab ranges together so each slab's sum keeps the
 // reference's sub-ray order.
 template <int VT>
-__global__ void __launch_bounds__(256) k_slicer_fused(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
+__global__ void __launch_bounds__(256, 3) k_slicer_fused(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
                                                       size_t img_stride, size_t pitchE, SlabTable slabs, int x0, int y0,
                                                       int x1, int y1) {
   const int lane = threadIdx.x & 31;

@@ -54,6 +54,8 @@ NTHREADS = int(os.environ.get("ORACLE_THREADS", os.cpu_count() or 1))
 
 def addr(a: np.ndarray):
     """Pointer that keeps the (possibly temporary) array alive for the call."""
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("oracle arrays must be C-contiguous")
     return a.ctypes.data_as(C.c_void_p)
 
 

@@ -1,0 +1,52 @@
+"""Build oracle/_ref/libref_kernels.so: the reference's kernel sources, host-compiled.
+
+Recipe (TEST INFRASTRUCTURE): every wrapper in oracle/ref_shim/ includes one
+of the reference's .cu files from its place in the reference tree
+(src/EmSART/cuda_kernels/, read-only, not copied). g++ compiles it for the
+host against the CUDA-execution shim in oracle/ref_shim/ (esb_ref_shim.h and
+the stand-in headers in oracle/ref_shim/include/). The shared library goes to
+oracle/_ref/, which git ignores. It is used only to pin the oracle against
+the reference's own kernel code. Needs the reference tree (REF_ROOT, default
+/root/reference); without it the build is skipped.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+SHIM = HERE / "ref_shim"
+OUT = HERE / "_ref" / "libref_kernels.so"
+REF_ROOT = Path(os.environ.get("REF_ROOT", "/root/reference"))
+KERNELS = REF_ROOT / "src" / "EmSART" / "cuda_kernels"
+UNITS = ["ref_runtime.cpp", "ref_fp.cpp", "ref_slicer.cpp", "ref_compare.cpp", "ref_bp.cpp", "ref_square.cpp",
+         "ref_ctf.cpp", "ref_wbp.cpp"]
+
+
+def available() -> bool:
+    return KERNELS.is_dir()
+
+
+def build(force: bool = False, verbose: bool = False) -> Path | None:
+    if not available():
+        if verbose:
+            print(f"reference kernels not found at {KERNELS}: skipping oracle/_ref", flush=True)
+        return OUT if OUT.exists() else None
+    OUT.parent.mkdir(exist_ok=True)
+    srcs = [SHIM / u for u in UNITS]
+    deps = srcs + list(SHIM.glob("*.h")) + list((SHIM / "include").glob("*.h"))
+    if not force and OUT.exists() and all(OUT.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return OUT
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-pthread",
+           "-w", "-D__CUDACC__", "-I", str(SHIM / "include"), "-I", str(SHIM), "-I", str(KERNELS),
+           *map(str, srcs), "-o", str(OUT)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

@@ -1,0 +1,33 @@
+// Reference kernels `slicer` and `volTraversalLength` (ForwardProjectionSlicer.cu), host-compiled.
+#include "ref_launch.h"
+namespace ref_sl {
+ESB_REF_USING
+#include "ForwardProjectionSlicer.cu"
+}
+
+extern "C" int ref_slicer(const RefGeom* g, const float* vol, int W, int H, float* proj, float tmin, float tmax,
+                          int weight8, int nthreads) {
+  ESB_REF_SET_CONSTANTS(ref_sl, *g, false);
+  EsbSoftTexture t;
+  t.data = vol;
+  t.dims = 3;
+  t.nx = (int)g->dim[0];
+  t.ny = (int)g->dim[1];
+  t.nz = (int)g->dim[2];
+  t.weight8 = weight8;
+  const CUtexObject obj = (CUtexObject)(uintptr_t)&t;
+  const size_t stride = (size_t)W * sizeof(float);
+  esb_grid(dim3((W + 31) / 32, (H + 7) / 8), dim3(32, 8), nthreads, [&]() {
+    ref_sl::slicer(W, H, stride, proj, tmin, tmax, obj, make_int2(0, 0), make_int2(W, H));
+  });
+  return 0;
+}
+
+extern "C" int ref_vol_traversal_length(const RefGeom* g, int W, int H, float* dist, int nthreads) {
+  ESB_REF_SET_CONSTANTS(ref_sl, *g, false);
+  const size_t stride = (size_t)W * sizeof(float);
+  esb_grid(dim3((W + 31) / 32, (H + 7) / 8), dim3(32, 8), nthreads, [&]() {
+    ref_sl::volTraversalLength(W, H, stride, dist, make_int2(0, 0), make_int2(W, H));
+  });
+  return 0;
+}
