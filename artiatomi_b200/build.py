@@ -31,6 +31,7 @@ UNITS = [
     ("esb_projector.cu", ["--fmad=false"]),
     ("esb_projector_fast.cu", []),
     ("esb_backprojector_fast.cu", []),
+    ("esb_subvolume.cu", []),
     ("esb_image.cu", ["--fmad=false"]),
     ("esb_api.cu", []),
     ("esb_noalloc.cu", []),

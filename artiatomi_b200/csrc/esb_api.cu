@@ -6,11 +6,13 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
 #include "esb_device.cuh"
 #include "esb_internal.h"
+#include "esb_subvolume.cuh"
 
 namespace esb {
 
@@ -337,6 +339,7 @@ struct esb_reconstructor {
   PhaseTimer timers[4];
   float* slab_imgs = nullptr;  // per-slab images of the fused CTF paths
   size_t slab_cap = 0;         // capacity in images
+  SubvolBatch batch;           // tables of the batched sub-volume launch
 };
 
 // Brackets a phase of launches with events when timing is enabled.
@@ -385,6 +388,7 @@ static void rec_free(esb_reconstructor* r) {
   cudaFree(r->slab_imgs);
   r->slab_imgs = nullptr;
   r->slab_cap = 0;
+  subvol_batch_free(r->batch);
 }
 
 extern "C" {
@@ -794,11 +798,65 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
   if (!r || !full_vol || !sub_geoms || !pair_geoms || !boxes || !projections || !index_list || n_particles < 0 ||
       proj_count < 0)
     return fail(ESB_ERR_INVALID_ARGUMENT, "esb_subvolume_wbp: invalid argument");
-  (void)batched;
   const esb_recon_config& cf = r->cfg;
   const int W = cf.proj_x, H = cf.proj_y, np = cf.n_proj;
   const size_t img = (size_t)W * H;
   int rc;
+  for (int ii = 0; ii < proj_count; ++ii)
+    if (index_list[ii] < 0 || index_list[ii] >= np)
+      return fail(ESB_ERR_INVALID_ARGUMENT, "esb_subvolume_wbp: index out of range");
+  if (batched && cf.variant == ESB_VARIANT_FAST && n_particles > 0 && proj_count > 0) {
+    std::vector<KConst> consts((size_t)n_particles * proj_count);
+    std::vector<unsigned char> act((size_t)n_particles * proj_count);
+    for (int p = 0; p < n_particles; ++p)
+      for (int ii = 0; ii < proj_count; ++ii) {
+        const size_t pair = (size_t)p * np + index_list[ii];
+        consts[(size_t)p * proj_count + ii] = rec_const(r, pair_geoms[pair], sub_geoms[p], 1);
+        act[(size_t)p * proj_count + ii] = active ? (active[pair] != 0) : 1;
+      }
+    if (subvol_batchable(n_particles, boxes, consts.data(), proj_count)) {
+      ESB_CK(subvol_batch_build(r->batch, n_particles, boxes, consts.data(), act.data(), proj_count, cf.oversampling,
+                                r->stream), "esb_subvolume_wbp");
+      if (!cf.ctf_mode) {
+        // all projections of the list resident (transposed), a chunk of up
+        // to 4 GiB of images per persistent launch
+        const int chunk = (int)std::max<size_t>(1, std::min<size_t>(proj_count, ((size_t)4 << 30) / (img * 4)));
+        if ((rc = rec_slab_capacity(r, chunk))) return rc;
+        SlabTable none;
+        none.count = 0;
+        for (int t0 = 0; t0 < proj_count; t0 += chunk) {
+          const int nt = std::min(chunk, proj_count - t0);
+          for (int t = 0; t < nt; ++t)
+            ESB_CK(launch_transpose(projections + (size_t)index_list[t0 + t] * img, W, H, W, r->slab_imgs + t * img,
+                                    r->stream), "esb_subvolume_wbp");
+          PhaseScope ps(r, 1);
+          ESB_CK(subvol_batch_launch(r->batch, t0, nt, r->slab_imgs, img, none, W, H, cf.oversampling, 0, r->stream),
+                 "esb_subvolume_wbp");
+        }
+        return ok();
+      }
+      static const int none[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int ii = 0; ii < proj_count; ++ii) {
+        const int index = index_list[ii];
+        SlabTable T;
+        if ((rc = rec_slab_table(r, full_vol, index, T))) return rc;
+        if ((rc = rec_slab_capacity(r, T.count))) return rc;
+        for (int k = 0; k < T.count; ++k) {
+          float dmin, dmax;
+          esb_defocus_min_max(T.bound[k], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
+                              cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
+                              cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
+          if ((rc = rec_ctf_chain(r, const_cast<float*>(projections + (size_t)index * img), 0, none, index, dmin, dmax,
+                                  0, r->slab_imgs + k * img, nullptr, 0, none, 1)))
+            return rc;
+        }
+        PhaseScope ps(r, 1);
+        ESB_CK(subvol_batch_launch(r->batch, ii, 1, r->slab_imgs, img, T, W, H, cf.oversampling, 1, r->stream),
+               "esb_subvolume_wbp");
+      }
+      return ok();
+    }
+  }
   // EmSartSubVolumes.cpp:626-683 with Reconstructor.cpp:893-914 / 975-1033
   for (int ii = 0; ii < proj_count; ++ii) {
     const int index = index_list[ii];

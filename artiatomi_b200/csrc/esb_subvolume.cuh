@@ -1,0 +1,43 @@
+// Host interface of the batched sub-volume back-projection (esb_subvolume.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "esb_device.cuh"
+
+namespace esb {
+
+// Device tables of one batched call: the work list (blocks of 128 voxel
+// quads of one particle), the particles' boxes and the kernel constants of
+// every (particle, list position) pair. Kept by the reconstructor and grown
+// on demand, so that repeated calls allocate nothing.
+struct SubvolBatch {
+  void* dev = nullptr;
+  size_t cap = 0;
+  std::vector<unsigned char> host;  // staging copy of the tables
+  size_t off_parts = 0, off_pairs = 0;
+  int n_work = 0;
+  int n_list = 0;
+};
+
+// True when every box can be updated with aligned float4 accesses (x extent a
+// multiple of 4, 16-byte aligned pointer): the batched kernel's layout.
+bool subvol_batchable(int n_particles, float* const* boxes, const KConst* consts, int n_list);
+
+// consts/active: [n_particles][n_list] for the list positions of one call;
+// active may be NULL (all pairs active).
+cudaError_t subvol_batch_build(SubvolBatch& b, int n_particles, float* const* boxes, const KConst* consts,
+                               const unsigned char* active, int n_list, int os, cudaStream_t st);
+
+// Adds list positions [t0, t0 + nt) to every box. Without slabs
+// (slabs.count == 0) position t reads image imgs + (t - t0) * img_stride;
+// with slabs each quad reads the image of its slab. Images are transposed
+// ([x][y]).
+cudaError_t subvol_batch_launch(const SubvolBatch& b, int t0, int nt, const float* imgs, size_t img_stride,
+                                const SlabTable& slabs, int pw, int ph, int os, int linear, cudaStream_t st);
+
+void subvol_batch_free(SubvolBatch& b);
+
+}  // namespace esb

@@ -206,20 +206,16 @@ def test_fast_sart_ctf():
         assert e <= tol, (prec, e)
 
 
-@pytest.mark.parametrize("ctf", [False, True])
-def test_fast_subvolume_wbp(ctf):
+def _subvolume_case(ctf, sizes, n=7, seed=31):
     import artiatomi_b200 as E
     from artiatomi_b200 import _lib as L
     from oracle import geometry as G
-    from oracle.driver import OracleReconstructor
 
     W = H = 96
-    n = 7
     tilt = np.linspace(-60, 60, n).astype(np.float32)
-    rng = np.random.default_rng(31)
+    rng = np.random.default_rng(seed)
     projs = rng.normal(size=(n, H, W)).astype(np.float32)
     full, fo = E.volume_geometry((96, 96, 40)), G.volume_geometry((96, 96, 40))
-    sizes = [16, 24, 16, 32]
     pos = rng.uniform(20, 76, size=(len(sizes), 3))
     pos[:, 2] = rng.uniform(10, 30, len(sizes))
     shifts = rng.uniform(-1.5, 1.5, size=(len(sizes), n, 2)).astype(np.float32)
@@ -235,15 +231,69 @@ def test_fast_subvolume_wbp(ctf):
     defocus = np.stack([np.full(n, 3000.0), np.full(n, 3100.0), np.full(n, 20.0)], 1).astype(np.float32).ravel()
     cfgd = dict(oversampling=2, ctf_mode=ctf, pixel_size_nm=0.27, ctf_slice_thickness_nm=4.0,
                 ctf_beta_fac=(10.0, 0.0, 0.008, 0.0))
-    pg = E.projection_geometry(E.Markers(tilt), W, H)
-    rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **cfgd), pg, tilt, defocus if ctf else None)
-    boxes = [cuda(np.zeros((s, s, s), np.float32)) for s in sizes]
-    il = np.arange(n, dtype=np.int32)
-    rec.subvolume_wbp(full, sub, pair, boxes, cuda(projs), il)
-    orc = OracleReconstructor(cfgd, W, H, G.projection_geometry(tilt, width=W, height=H), tilt,
-                              defocus if ctf else None, precision=1)
-    bo = [np.zeros((s, s, s), np.float32) for s in sizes]
-    orc.subvolume_wbp(fo, subo, pair_o, bo, projs, il)
-    for b, o in zip(boxes, bo):
-        e = rel_l2(host(b), o)
+    return dict(W=W, H=H, n=n, tilt=tilt, projs=projs, full=full, fo=fo, sub=sub, subo=subo, pair=pair,
+                pair_o=pair_o, defocus=defocus if ctf else None, cfgd=cfgd, shifts=shifts, sizes=sizes)
+
+
+def _subvolume_gpu(c, batched, index_list, active=None):
+    import artiatomi_b200 as E
+
+    W, H, n = c["W"], c["H"], c["n"]
+    pg = E.projection_geometry(E.Markers(c["tilt"]), W, H)
+    rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **c["cfgd"]), pg, c["tilt"], c["defocus"])
+    boxes = [cuda(np.zeros((s, s, s), np.float32)) for s in c["sizes"]]
+    rec.subvolume_wbp(c["full"], c["sub"], c["pair"], boxes, cuda(c["projs"]), index_list, active=active,
+                      batched=batched)
+    return [host(b) for b in boxes]
+
+
+def _subvolume_oracle(c, index_list, active=None):
+    from oracle import geometry as G
+    from oracle.driver import OracleReconstructor
+
+    W, H = c["W"], c["H"]
+    orc = OracleReconstructor(c["cfgd"], W, H, G.projection_geometry(c["tilt"], width=W, height=H), c["tilt"],
+                              c["defocus"], precision=1)
+    bo = [np.zeros((s, s, s), np.float32) for s in c["sizes"]]
+    orc.subvolume_wbp(c["fo"], c["subo"], c["pair_o"], bo, c["projs"], index_list, active=active)
+    return bo
+
+
+@pytest.mark.parametrize("ctf,batched", [(False, False), (True, False), (False, True), (True, True)])
+def test_fast_subvolume_wbp(ctf, batched):
+    c = _subvolume_case(ctf, [16, 24, 16, 32])
+    il = np.arange(c["n"], dtype=np.int32)
+    got = _subvolume_gpu(c, batched, il)
+    for b, o in zip(got, _subvolume_oracle(c, il)):
+        e = rel_l2(b, o)
         assert e <= 1e-4, e
+
+
+@pytest.mark.parametrize("ctf", [False, True])
+def test_batched_subvolume_matches_per_particle(ctf):
+    """One persistent launch over mixed boxes matches one launch per particle
+    per tilt: the same per-voxel sums added in the same order (tilts in list
+    order, inactive pairs skipped). The two kernels are compiled separately
+    and may contract multiply-adds differently, so agreement is to float
+    rounding, not bit-exact."""
+    c = _subvolume_case(ctf, [16, 24, 32, 48, 16, 24], n=9, seed=5)
+    il = np.random.default_rng(1).permutation(c["n"]).astype(np.int32)
+    active = (np.linalg.norm(c["shifts"], axis=2) < 1.5).astype(np.uint8)
+    plain = _subvolume_gpu(c, False, il, active)
+    batch = _subvolume_gpu(c, True, il, active)
+    for a, b in zip(plain, batch):
+        assert np.abs(a).sum() > 0
+        assert rel_l2(b, a) <= 1e-5
+        assert np.abs(b - a).max() <= 1e-5 * np.abs(a).max()
+    for b, o in zip(batch, _subvolume_oracle(c, il, active)):
+        assert rel_l2(b, o) <= 1e-4
+
+
+def test_batched_subvolume_ragged_box_runs_per_particle():
+    """A box whose x extent is not a multiple of 4 cannot take the batched
+    kernel's float4 layout; the call then runs the per-particle launches."""
+    c = _subvolume_case(False, [16, 18, 24], n=5, seed=8)
+    il = np.arange(c["n"], dtype=np.int32)
+    got = _subvolume_gpu(c, True, il)
+    for b, o in zip(got, _subvolume_oracle(c, il)):
+        assert rel_l2(b, o) <= 1e-4

@@ -138,9 +138,6 @@ def test_subvolume_wbp(ctf, batched):
     shifts = rng.uniform(-1.5, 1.5, size=(len(sizes), n, 2)).astype(np.float32)
     sub = [E.subvolume_geometry(s, 1.0, full, p) for s, p in zip(sizes, pos)]
     subo = [G.subvolume_geometry(s, 1.0, fo, p) for s, p in zip(sizes, pos)]
-    pair = (E.projection_geometry(E.Markers(tilt), W, H) * 0).__class__ if False else None
-    import ctypes as C
-
     from artiatomi_b200 import _lib as L
 
     pair = (L.ProjGeom * (len(sizes) * n))()
