@@ -41,21 +41,26 @@ struct BpGeom {
   float U0, V0;
   float3 u, v;   // detector axes (world per pixel)
   float3 inv_n;  // 1 / ray direction per axis
+  // entry and exit face offsets per axis: the ray c + d + tau*n enters the
+  // slab |p - c| <= hb of axis j at tau = (cn_j - d_j) / n_j and leaves it
+  // at (cf_j - d_j) / n_j (cn = -hb, cf = +hb for n_j > 0, swapped else)
+  float3 cn, cf;
   float hu, hv;  // half extent of a voxel's shadow in pixels
   float3 hb;     // half voxel size
-  int exact_grid;  // oversampling is a power of two: the recurrence is exact
+  int exact_grid;      // oversampling is a power of two: the recurrence is exact
+  int aniso_identity;  // no magnification anisotropy: samples read at (px, py)
 };
 
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 
 // Chord of the line c + d + tau*n through the box |p - c| <= hb per axis.
-__device__ __forceinline__ float chord(float3 d, float3 inv_n, float3 hb) {
-  float t0x = (-hb.x - d.x) * inv_n.x, t1x = (hb.x - d.x) * inv_n.x;
-  float t0y = (-hb.y - d.y) * inv_n.y, t1y = (hb.y - d.y) * inv_n.y;
-  float t0z = (-hb.z - d.z) * inv_n.z, t1z = (hb.z - d.z) * inv_n.z;
-  float tin = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
-  float tout = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
+// With the entry/exit faces resolved by the sign of n, each axis costs two
+// subtractions and two products; a zero component (1/n infinite) leaves the
+// axis unconstrained while |d| < hb and empties the chord when |d| > hb.
+__device__ __forceinline__ float chord(float dx, float dy, float dz, const BpGeom& g) {
+  const float tin = fmaxf(fmaxf((g.cn.x - dx) * g.inv_n.x, (g.cn.y - dy) * g.inv_n.y), (g.cn.z - dz) * g.inv_n.z);
+  const float tout = fminf(fminf((g.cf.x - dx) * g.inv_n.x, (g.cf.y - dy) * g.inv_n.y), (g.cf.z - dz) * g.inv_n.z);
   return tout - tin;
 }
 
@@ -120,9 +125,28 @@ __device__ __forceinline__ float first_sample(int lo, float inv, float a, bool e
 }
 
 
+// Image sample without clamping, for samples known to lie inside the image
+// (the generic path's clamps are then no-ops): texel (ix, iy) at
+// img + ix * sx + iy * sy.
+__device__ __forceinline__ float sample_interior(const float* __restrict__ img, size_t sx, size_t sy, float x,
+                                                 float y, bool linear) {
+  if (!linear) return __ldg(img + (size_t)(int)x * sx + (size_t)(int)y * sy);  // x, y >= 0
+  const float xb = x - 0.5f, yb = y - 0.5f;
+  const float fx = floorf(xb), fy = floorf(yb);
+  const float a = xb - fx, b = yb - fy;
+  const float* p = img + (size_t)(int)fx * sx + (size_t)(int)fy * sy;
+  const float t00 = __ldg(p), t10 = __ldg(p + sx), t01 = __ldg(p + sy), t11 = __ldg(p + sx + sy);
+  return (1.0f - b) * ((1.0f - a) * t00 + a * t10) + b * ((1.0f - a) * t01 + a * t11);
+}
+
 // sum(sample*chord) and sum(chord) of voxel (x + i, y, z) of the quad at
 // (x, y, z) whose macro-cell rectangle is pb*, over the reference's sub-pixel
 // recurrence restricted to the voxel's shadow.
+//
+// Samples run over [pbx, pby) x [pbz, pbw) with pby <= pw - 1 and
+// pbw <= ph - 1, so a nearest-texel read never leaves the image and a
+// bilinear read only does so below a lower edge: with no anisotropy the
+// clamps are skipped unless pbx or pbz is 0 under bilinear interpolation.
 __device__ __forceinline__ void voxel_sums(const KConst& k, const BpGeom& g, const float* __restrict__ img, int pw,
                                            int ph, size_t pitchE, int os, float inv, bool linear, bool transposed,
                                            int x, int y, int z, int pbx, int pby, int pbz, int pbw, float& acc,
@@ -133,21 +157,35 @@ __device__ __forceinline__ void voxel_sums(const KConst& k, const BpGeom& g, con
   const float vc = g.V.x * cx + g.V.y * cy + g.V.z * cz + g.V0;
   const float ua = uc - g.hu, ub = uc + g.hu, va = vc - g.hv, vb = vc + g.hv;
   const bool exact = g.exact_grid != 0;
+  const bool fast = g.aniso_identity != 0 && (!linear || (pbx >= 1 && pbz >= 1));
+  const size_t sx = transposed ? (size_t)ph : 1, sy = transposed ? 1 : pitchE;
   float a = 0.f, da = 0.f;
   const float py0 = first_sample(pbz, inv, va, exact, os), px0 = first_sample(pbx, inv, ua, exact, os);
+  const float du0 = px0 - uc;
+  // in-plane offset d = du * u + dv * v, advanced by inv * u per sample
+  const float ix = inv * g.u.x, iy = inv * g.u.y, iz = inv * g.u.z;
 #pragma unroll 1
   for (float py = py0; py < (float)pbw && py <= vb; py = fadd(py, inv)) {
+    const float dv = py - vc;
+    float dx = du0 * g.u.x + dv * g.v.x, dy = du0 * g.u.y + dv * g.v.y, dz = du0 * g.u.z + dv * g.v.z;
 #pragma unroll 1
     for (float px = px0; px < (float)pby && px <= ub; px = fadd(px, inv)) {
-      const float du = px - uc, dv = py - vc;
-      const float3 d = make_float3(du * g.u.x + dv * g.v.x, du * g.u.y + dv * g.v.y, du * g.u.z + dv * g.v.z);
-      const float L = chord(d, g.inv_n, g.hb);
+      const float L = chord(dx, dy, dz, g);
       if (L > 0.0f) {
-        const float xA = k.anisoInv[0] * px + k.anisoInv[1] * py + k.anisoInv[2];
-        const float yA = k.anisoInv[3] * px + k.anisoInv[4] * py + k.anisoInv[5];
-        a += sample_image(img, pw, ph, pitchE, xA, yA, linear, transposed) * L;
+        float s;
+        if (fast) {
+          s = sample_interior(img, sx, sy, px, py, linear);
+        } else {
+          const float xA = k.anisoInv[0] * px + k.anisoInv[1] * py + k.anisoInv[2];
+          const float yA = k.anisoInv[3] * px + k.anisoInv[4] * py + k.anisoInv[5];
+          s = sample_image(img, pw, ph, pitchE, xA, yA, linear, transposed);
+        }
+        a += s * L;
         da += L;
       }
+      dx += ix;
+      dy += iy;
+      dz += iz;
     }
   }
   acc = a;
@@ -164,11 +202,18 @@ inline BpGeom make_geom(const KConst& k, int os) {
   g.v = k.v;
   g.inv_n = make_float3(1.0f / k.n.x, 1.0f / k.n.y, 1.0f / k.n.z);
   g.hb = make_float3(0.5f * k.vs.x, 0.5f * k.vs.y, 0.5f * k.vs.z);
+  g.cn = make_float3(signbit(g.inv_n.x) ? g.hb.x : -g.hb.x, signbit(g.inv_n.y) ? g.hb.y : -g.hb.y,
+                     signbit(g.inv_n.z) ? g.hb.z : -g.hb.z);
+  g.cf = make_float3(-g.cn.x, -g.cn.y, -g.cn.z);
   // shadow half extents, widened by a hair so that samples on the edge of a
   // shadow are tested (their chord decides)
   g.hu = 0.5f * (fabsf(g.U.x) * k.vs.x + fabsf(g.U.y) * k.vs.y + fabsf(g.U.z) * k.vs.z) * 1.0001f + 1e-5f;
   g.hv = 0.5f * (fabsf(g.V.x) * k.vs.x + fabsf(g.V.y) * k.vs.y + fabsf(g.V.z) * k.vs.z) * 1.0001f + 1e-5f;
   g.exact_grid = (os & (os - 1)) == 0;
+  static const float ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  g.aniso_identity = 1;
+  for (int i = 0; i < 9; ++i)
+    if (k.anisoInv[i] != ident[i]) g.aniso_identity = 0;
   return g;
 }
 
