@@ -66,6 +66,7 @@ SZ = C.c_size_t
 _SIGS = {
     "esb_last_error": ([], C.c_char_p),
     "esb_version": ([], I),
+    "esb_kernel_launches": ([], C.c_ulonglong),
     "esb_projection_geometry": ([I, I, I, P, P, P, P, P, P, C.POINTER(TiltConfig), P], I),
     "esb_volume_geometry": ([P, I, I, P, P, C.POINTER(VolGeom)], I),
     "esb_subvolume_geometry": ([I, F, C.POINTER(VolGeom), P, P, C.POINTER(VolGeom)], I),

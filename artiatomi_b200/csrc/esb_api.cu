@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -44,6 +45,12 @@ cudaError_t launch_square_to_image(const float* sq, int maxsize, size_t shift, f
                                    size_t pitchE, float* out, float* accum, int apply_crop, float2 cut, float2 dim,
                                    const int* p, cudaStream_t st, int transpose_out);
 cudaError_t launch_transpose(const float* in, int w, int h, size_t pitchE, float* out, cudaStream_t st);
+cudaError_t launch_square_to_image_batch(const float* sq, int count, int maxsize, size_t shift, float inv_norm, int pw,
+                                         int ph, size_t pitchE, float* out, size_t out_stride, int transpose_out,
+                                         cudaStream_t st);
+cudaError_t launch_ctf_slabs(const float* in, float* out, size_t out_stride, int n, const CtfConst& k,
+                             const CtfSlabs& slabs_nm, float angle_deg, int applyForFP, int phaseFlip, float wiener,
+                             float4 beta, cudaStream_t st);
 CtfConst make_ctf_const(int n, float cs_mm, float voltage_kv, float amp_contrast, float pixel_size_nm);
 cudaError_t launch_ctf(float* spec, int n, const CtfConst& k, float d0_nm, float d1_nm, float angle_deg, int applyForFP,
                        int phaseFlip, float wiener, float4 beta, cudaStream_t st);
@@ -54,6 +61,9 @@ cudaError_t launch_convert(const void* vol, int vt, long n, float* out, float si
 cudaError_t launch_store(const float* in, long n, void* vol, int vt, cudaStream_t st);
 
 static thread_local std::string g_last_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 int fail(int code, const std::string& msg) {
@@ -104,6 +114,7 @@ extern "C" {
 
 const char* esb_last_error(void) { return g_last_error.c_str(); }
 int esb_version(void) { return 100; }
+unsigned long long esb_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int esb_fp(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y, float* proj, float* dist,
            size_t pitch, int roi_x0, int roi_y0, int roi_x1, int roi_y1, void* stream) {
@@ -340,6 +351,13 @@ struct esb_reconstructor {
   float* slab_imgs = nullptr;  // per-slab images of the fused CTF paths
   size_t slab_cap = 0;         // capacity in images
   SubvolBatch batch;           // tables of the batched sub-volume launch
+  // filtered spectra and squares of a chunk of CTF slabs, with a batched
+  // C2R plan per chunk size
+  float* spec_batch = nullptr;
+  float* sq_batch = nullptr;
+  int batch_slabs = 0;
+  cufftHandle c2r_many[ESB_CTF_SLAB_BATCH + 1] = {};
+  bool c2r_many_ok[ESB_CTF_SLAB_BATCH + 1] = {};
 };
 
 // Brackets a phase of launches with events when timing is enabled.
@@ -389,6 +407,15 @@ static void rec_free(esb_reconstructor* r) {
   r->slab_imgs = nullptr;
   r->slab_cap = 0;
   subvol_batch_free(r->batch);
+  cudaFree(r->spec_batch);
+  cudaFree(r->sq_batch);
+  r->spec_batch = r->sq_batch = nullptr;
+  r->batch_slabs = 0;
+  for (int i = 0; i <= ESB_CTF_SLAB_BATCH; ++i)
+    if (r->c2r_many_ok[i]) {
+      cufftDestroy(r->c2r_many[i]);
+      r->c2r_many_ok[i] = false;
+    }
 }
 
 extern "C" {
@@ -442,6 +469,8 @@ int esb_reconstructor_set_stream(esb_reconstructor* rec, void* stream) {
   if (rec->plans) {
     ESB_FFT(cufftSetStream(rec->r2c, rec->stream), "esb_reconstructor_set_stream");
     ESB_FFT(cufftSetStream(rec->c2r, rec->stream), "esb_reconstructor_set_stream");
+    for (int i = 0; i <= ESB_CTF_SLAB_BATCH; ++i)
+      if (rec->c2r_many_ok[i]) ESB_FFT(cufftSetStream(rec->c2r_many[i], rec->stream), "esb_reconstructor_set_stream");
   }
   return ok();
 }
@@ -573,6 +602,64 @@ static int rec_slab_capacity(esb_reconstructor* r, int count) {
   const size_t bytes = (size_t)count * r->cfg.proj_x * r->cfg.proj_y * sizeof(float);
   ESB_CK(cudaMalloc(&r->slab_imgs, bytes), "slab images");
   r->slab_cap = count;
+  return ESB_OK;
+}
+
+// Wiener-filtered slab images of prepared projection `index` for the
+// sub-volume paths, into slab_imgs (transposed). The reference pads,
+// transforms, filters and transforms back the same projection once per slab
+// (Reconstructor.cpp:975-1004, no crop). Here the projection is padded and
+// transformed once; each chunk of up to ESB_CTF_SLAB_BATCH slabs gets its
+// filtered spectra in one launch, one batched C2R and one batched
+// scale + window + transpose.
+static int rec_subvol_slab_images(esb_reconstructor* r, const esb_vol_geom* full_vol, const float* proj, int index,
+                                  SlabTable& T) {
+  const esb_recon_config& cf = r->cfg;
+  const int W = cf.proj_x, H = cf.proj_y, N = r->N;
+  int rc;
+  if ((rc = rec_slab_table(r, full_vol, index, T))) return rc;
+  if ((rc = rec_slab_capacity(r, T.count))) return rc;
+  const int want = std::min(T.count, ESB_CTF_SLAB_BATCH);
+  const size_t spec = (size_t)(N / 2 + 1) * N * 2, sq = (size_t)N * N;
+  if (want > r->batch_slabs) {
+    ESB_CK(cudaStreamSynchronize(r->stream), "CTF slab images");
+    cudaFree(r->spec_batch);
+    cudaFree(r->sq_batch);
+    r->spec_batch = r->sq_batch = nullptr;
+    r->batch_slabs = 0;
+    ESB_CK(cudaMalloc(&r->spec_batch, (size_t)want * spec * sizeof(float)), "CTF slab images");
+    ESB_CK(cudaMalloc(&r->sq_batch, (size_t)want * sq * sizeof(float)), "CTF slab images");
+    r->batch_slabs = want;
+  }
+  static const int none[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const size_t img = (size_t)W * H;
+  PhaseScope ps(r, 2);
+  ESB_CK(launch_crop_to_square(W, H, W, const_cast<float*>(proj), 0, make_float2(0.f, 0.f), make_float2(0.f, 0.f), none,
+                               N, r->square_d, r->borderX, r->borderY, r->stream), "CTF slab images");
+  ESB_FFT(cufftExecR2C(r->r2c, (cufftReal*)r->square_d, (cufftComplex*)r->fft_d), "CTF slab images R2C");
+  const float4 beta = make_float4(cf.ctf_beta_fac[0], cf.ctf_beta_fac[1], cf.ctf_beta_fac[2], cf.ctf_beta_fac[3]);
+  for (int c0 = 0; c0 < T.count; c0 += ESB_CTF_SLAB_BATCH) {
+    const int cnt = std::min(ESB_CTF_SLAB_BATCH, T.count - c0);
+    CtfSlabs S;
+    S.count = cnt;
+    for (int j = 0; j < cnt; ++j)
+      esb_defocus_min_max(T.bound[c0 + j], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
+                          cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
+                          cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &S.d0[j], &S.d1[j]);
+    ESB_CK(launch_ctf_slabs(r->fft_d, r->spec_batch, spec, N, r->ctfk, S, r->defocus[3 * index + 2], 0,
+                            cf.phase_flip_only, cf.wiener_noise_level, beta, r->stream), "CTF slab images");
+    if (!r->c2r_many_ok[cnt]) {
+      int dims[2] = {N, N};
+      ESB_FFT(cufftPlanMany(&r->c2r_many[cnt], 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, cnt),
+              "CTF slab images plan");
+      r->c2r_many_ok[cnt] = true;
+      ESB_FFT(cufftSetStream(r->c2r_many[cnt], r->stream), "CTF slab images plan");
+    }
+    ESB_FFT(cufftExecC2R(r->c2r_many[cnt], (cufftComplex*)r->spec_batch, (cufftReal*)r->sq_batch),
+            "CTF slab images C2R");
+    ESB_CK(launch_square_to_image_batch(r->sq_batch, cnt, N, r->squareShift, 1.0f / ((float)N * (float)N), W, H, W,
+                                        r->slab_imgs + (size_t)c0 * img, img, 1, r->stream), "CTF slab images");
+  }
   return ESB_OK;
 }
 
@@ -835,21 +922,10 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
         }
         return ok();
       }
-      static const int none[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       for (int ii = 0; ii < proj_count; ++ii) {
         const int index = index_list[ii];
         SlabTable T;
-        if ((rc = rec_slab_table(r, full_vol, index, T))) return rc;
-        if ((rc = rec_slab_capacity(r, T.count))) return rc;
-        for (int k = 0; k < T.count; ++k) {
-          float dmin, dmax;
-          esb_defocus_min_max(T.bound[k], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
-                              cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
-                              cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
-          if ((rc = rec_ctf_chain(r, const_cast<float*>(projections + (size_t)index * img), 0, none, index, dmin, dmax,
-                                  0, r->slab_imgs + k * img, nullptr, 0, none, 1)))
-            return rc;
-        }
+        if ((rc = rec_subvol_slab_images(r, full_vol, projections + (size_t)index * img, index, T))) return rc;
         PhaseScope ps(r, 1);
         ESB_CK(subvol_batch_launch(r->batch, ii, 1, r->slab_imgs, img, T, W, H, cf.oversampling, 1, r->stream),
                "esb_subvolume_wbp");
@@ -892,18 +968,7 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
       // Wiener-filtered image per slab of the whole tomogram, then one launch
       // per particle that picks each quad's slab image by its depth
       SlabTable T;
-      if ((rc = rec_slab_table(r, full_vol, index, T))) return rc;
-      if ((rc = rec_slab_capacity(r, T.count))) return rc;
-      static const int none[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int k = 0; k < T.count; ++k) {
-        float dmin, dmax;
-        esb_defocus_min_max(T.bound[k], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
-                            cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
-                            cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
-        if ((rc = rec_ctf_chain(r, const_cast<float*>(proj), 0, none, index, dmin, dmax, 0, r->slab_imgs + k * img,
-                                nullptr, 0, none, 1)))
-          return rc;
-      }
+      if ((rc = rec_subvol_slab_images(r, full_vol, proj, index, T))) return rc;
       for (int p = 0; p < n_particles; ++p) {
         if (active && !active[(size_t)p * np + index]) continue;
         KConst c = rec_const(r, pair_geoms[(size_t)p * np + index], sub_geoms[p], 1);

@@ -86,9 +86,9 @@ cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float
   const float inv = 1.0f / (float)os;
   dim3 blk(32, 4, 1), grd((nq + 31) / 32, (ny + 3) / 4, nz);
   switch (vt) {
-    case ESB_VOXEL_F32: k_bp_fast<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); break;
-    case ESB_VOXEL_F16: k_bp_fast<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); break;
-    default: k_bp_fast<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); break;
+    case ESB_VOXEL_F32: k_bp_fast<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); ESB_COUNT_LAUNCH(); break;
+    case ESB_VOXEL_F16: k_bp_fast<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); ESB_COUNT_LAUNCH(); break;
+    default: k_bp_fast<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); ESB_COUNT_LAUNCH(); break;
   }
   return cudaGetLastError();
 }

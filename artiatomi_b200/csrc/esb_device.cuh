@@ -60,6 +60,17 @@ struct CtfConst {
   float cs, lambda, ampC, phaseC, freqStep, pixelcount;
 };
 
+// Every kernel launch of the library is counted (esb_kernel_launches).
+void count_launch();
+#define ESB_COUNT_LAUNCH() ::esb::count_launch()
+
+// Defocus ranges of up to ESB_CTF_SLAB_BATCH slabs filtered in one launch.
+#define ESB_CTF_SLAB_BATCH 16
+struct CtfSlabs {
+  int count;
+  float d0[ESB_CTF_SLAB_BATCH], d1[ESB_CTF_SLAB_BATCH];
+};
+
 template <int VT>
 struct Voxel;
 template <>

@@ -145,6 +145,18 @@ __global__ void k_square_to_image(const float* __restrict__ sq, int maxsize, siz
   if (accum) accum[i] += v;
 }
 
+// k_square_to_image without crop or accumulation for a stack of squares:
+// square blockIdx.z to image blockIdx.z.
+__global__ void k_square_to_image_batch(const float* __restrict__ sq, size_t sq_stride, int maxsize, size_t shift,
+                                        float inv_norm, int pw, int ph, size_t pitchE, float* __restrict__ out,
+                                        size_t out_stride, int transpose_out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= pw || y >= ph) return;
+  const float v = sq[blockIdx.z * sq_stride + shift + (size_t)y * maxsize + x] * inv_norm;
+  out[blockIdx.z * out_stride + (transpose_out ? (size_t)x * ph + y : (size_t)y * pitchE + x)] = v;
+}
+
 // out[x][y] = in[y][x] for a W x H image (32x32 tiles through shared memory).
 __global__ void k_transpose(const float* __restrict__ in, int w, int h, size_t pitchE, float* __restrict__ out) {
   __shared__ float tile[32][33];
@@ -203,6 +215,58 @@ __global__ void k_ctf(float2* __restrict__ spec, int n, CtfConst k, float d0, fl
     res.y = -res.y;
   }
   spec[i] = res;
+}
+
+// The `ctf` kernel applied to one spectrum for several defocus ranges at
+// once: out + k * out_stride = ctf(in, d0[k], d1[k]). The per-frequency
+// terms that do not depend on defocus are computed once; each output equals
+// what k_ctf would make of a copy of `in` (same expressions, same order).
+__global__ void k_ctf_slabs(const float2* __restrict__ in, float2* __restrict__ out, size_t out_stride, int n,
+                            CtfConst k, CtfSlabs slabs, float angle, int applyForFP, int phaseFlipOnly, float wiener,
+                            float4 beta) {
+  const unsigned x = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= (unsigned)(n / 2 + 1) || y >= (unsigned)n) return;
+  const float PI = 3.14159265358979323846f;
+  float xpos = (float)x, ypos = (float)y;
+  if (ypos > k.pixelcount * 0.5f) ypos = (k.pixelcount - ypos) * -1.0f;
+  float alpha = (xpos == 0.f) ? (PI * 0.5f) : atan2f(ypos, xpos);
+  float beta_ = alpha - angle;
+  const float c2 = (1.f - cosf(2.f * beta_));
+  float radius = sqrtf(xpos * xpos + ypos * ypos);
+  float length = radius * k.freqStep;
+  float L = k.lambda;
+  const float l = length / 100000000.0f;
+  const float e0 = expf(-beta.y * l - beta.z * l * l - beta.w * l * l * l);
+  const size_t i = (size_t)y * (n / 2 + 1) + x;
+  const float2 src = in[i];
+  for (int s = 0; s < slabs.count; ++s) {
+    const float d0 = slabs.d0[s], d1 = slabs.d1[s];
+    float defocus = d0 + c2 * (d1 - d0);
+    float m = (PI / 2.0f) * (k.cs * L * L * L * length * length * length * length - 2.f * defocus * L * length * length);
+    float nn = k.phaseC * sinf(m) + k.ampC * cosf(m);
+    float2 res = src;
+    if (applyForFP && radius > beta.x && !phaseFlipOnly) {
+      float e = fmaxf(e0, 0.01f);
+      float val = nn * e;
+      if (fabsf(val) < 0.0001f && val >= 0.f) val = 0.0001f;
+      if (fabsf(val) < 0.0001f && val < 0.f) val = -0.0001f;
+      res.x = res.x * -val;
+      res.y = res.y * -val;
+    }
+    if (!applyForFP && radius > beta.x && !phaseFlipOnly) {
+      float e = fmaxf(e0, wiener);
+      float val = nn * e;
+      float f = -val / (val * val + wiener);
+      res.x = res.x * f;
+      res.y = res.y * f;
+    }
+    if (phaseFlipOnly && nn >= 0.f) {
+      res.x = -res.x;
+      res.y = -res.y;
+    }
+    out[(size_t)s * out_stride + i] = res;
+  }
 }
 
 // Kernel `wbpWeighting` (wbpWeighting.cu:50-144).
@@ -304,7 +368,7 @@ static inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x
 cudaError_t launch_compare(int pw, int ph, size_t pitchE, const float* real, float* virt, const float* dist,
                            float realLength, float4 cut, float4 dim, float scale, cudaStream_t st) {
   dim3 b(32, 8);
-  k_compare<<<grid2(pw, ph, b), b, 0, st>>>(pw, ph, pitchE, real, virt, dist, realLength, cut, dim, scale);
+  k_compare<<<grid2(pw, ph, b), b, 0, st>>>(pw, ph, pitchE, real, virt, dist, realLength, cut, dim, scale); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -312,14 +376,14 @@ cudaError_t launch_crop_border(int pw, int ph, size_t pitchE, float* img, float2
                                cudaStream_t st) {
   dim3 b(32, 8);
   k_crop_border<<<grid2(pw, ph, b), b, 0, st>>>(pw, ph, pitchE, img, cut, dim, make_int2(p[0], p[1]),
-                                                 make_int2(p[2], p[3]), make_int2(p[4], p[5]), make_int2(p[6], p[7]));
+                                                 make_int2(p[2], p[3]), make_int2(p[4], p[5]), make_int2(p[6], p[7])); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
 cudaError_t launch_make_square(int pw, int ph, size_t strideE, const float* in, int maxsize, float* out, int bx,
                                int by, int mirrorY, int fillZero, cudaStream_t st) {
   dim3 b(32, 8);
-  k_make_square<<<grid2(maxsize, maxsize, b), b, 0, st>>>(pw, ph, maxsize, strideE, in, out, bx, by, mirrorY, fillZero);
+  k_make_square<<<grid2(maxsize, maxsize, b), b, 0, st>>>(pw, ph, maxsize, strideE, in, out, bx, by, mirrorY, fillZero); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -329,7 +393,7 @@ cudaError_t launch_crop_to_square(int pw, int ph, size_t pitchE, float* img, int
   k_crop_to_square<<<grid2(maxsize, maxsize, b), b, 0, st>>>(pw, ph, pitchE, img, apply_crop, cut, dim,
                                                             make_int2(p[0], p[1]), make_int2(p[2], p[3]),
                                                             make_int2(p[4], p[5]), make_int2(p[6], p[7]), maxsize, sq,
-                                                            bx, by);
+                                                            bx, by); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -339,13 +403,29 @@ cudaError_t launch_square_to_image(const float* sq, int maxsize, size_t shift, f
   dim3 b(32, 8);
   k_square_to_image<<<grid2(pw, ph, b), b, 0, st>>>(sq, maxsize, shift, inv_norm, pw, ph, pitchE, out, accum,
                                                     apply_crop, cut, dim, make_int2(p[0], p[1]), make_int2(p[2], p[3]),
-                                                    make_int2(p[4], p[5]), make_int2(p[6], p[7]), transpose_out);
+                                                    make_int2(p[4], p[5]), make_int2(p[6], p[7]), transpose_out); ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// k_square_to_image over `count` squares (stride maxsize^2) into `count`
+// images (stride out_stride), one launch per 65535 squares.
+cudaError_t launch_square_to_image_batch(const float* sq, int count, int maxsize, size_t shift, float inv_norm, int pw,
+                                         int ph, size_t pitchE, float* out, size_t out_stride, int transpose_out,
+                                         cudaStream_t st) {
+  dim3 b(32, 8);
+  for (int c0 = 0; c0 < count; c0 += 65535) {
+    dim3 g = grid2(pw, ph, b);
+    g.z = (unsigned)(count - c0 < 65535 ? count - c0 : 65535);
+    k_square_to_image_batch<<<g, b, 0, st>>>(sq + (size_t)c0 * maxsize * maxsize, (size_t)maxsize * maxsize, maxsize,
+                                              shift, inv_norm, pw, ph, pitchE, out + (size_t)c0 * out_stride,
+                                              out_stride, transpose_out); ESB_COUNT_LAUNCH();
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_transpose(const float* in, int w, int h, size_t pitchE, float* out, cudaStream_t st) {
   dim3 b(32, 8), g((w + 31) / 32, (h + 31) / 32);
-  k_transpose<<<g, b, 0, st>>>(in, w, h, pitchE, out);
+  k_transpose<<<g, b, 0, st>>>(in, w, h, pitchE, out); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -371,26 +451,42 @@ cudaError_t launch_ctf(float* spec, int n, const CtfConst& k, float d0_nm, float
   dim3 b(32, 8);
   float d0 = d0_nm * 0.000000001f, d1 = d1_nm * 0.000000001f;
   float ang = angle_deg / 180.0f * 3.14159265358979323846f;
-  k_ctf<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, k, d0, d1, ang, applyForFP, phaseFlip, wiener, beta);
+  k_ctf<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, k, d0, d1, ang, applyForFP, phaseFlip, wiener, beta); ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// out_stride: floats between output spectra (even: whole complex values).
+cudaError_t launch_ctf_slabs(const float* in, float* out, size_t out_stride, int n, const CtfConst& k,
+                             const CtfSlabs& slabs_nm, float angle_deg, int applyForFP, int phaseFlip, float wiener,
+                             float4 beta, cudaStream_t st) {
+  dim3 b(32, 8);
+  CtfSlabs sl = slabs_nm;
+  for (int i = 0; i < sl.count; ++i) {
+    sl.d0[i] = slabs_nm.d0[i] * 0.000000001f;
+    sl.d1[i] = slabs_nm.d1[i] * 0.000000001f;
+  }
+  float ang = angle_deg / 180.0f * 3.14159265358979323846f;
+  k_ctf_slabs<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((const float2*)in, (float2*)out, out_stride / 2, n, k, sl, ang,
+                                                    applyForFP, phaseFlip, wiener, beta); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
 cudaError_t launch_wbp_weighting(float* spec, int n, float psi_deg, int fm, cudaStream_t st) {
   dim3 b(32, 8);
   float a = -psi_deg / 180.0f * 3.14159265358979323846f;
-  k_wbp_weighting<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, (float)sin((double)a), (float)cos((double)a), fm);
+  k_wbp_weighting<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, (float)sin((double)a), (float)cos((double)a), fm); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
 cudaError_t launch_fourier_filter(float* spec, int n, float lp, float hp, float lps, float hps, cudaStream_t st) {
   dim3 b(32, 8);
-  k_fourier_filter<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, lp, hp, lps, hps);
+  k_fourier_filter<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, lp, hp, lps, hps); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
 cudaError_t launch_dose_weighting(float* spec, int n, float dose, float pixelsize, cudaStream_t st) {
   dim3 b(32, 8);
-  k_dose_weighting<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, dose, pixelsize);
+  k_dose_weighting<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, n, dose, pixelsize); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -398,9 +494,9 @@ cudaError_t launch_convert(const void* vol, int vt, long n, float* out, float si
   int blocks = (int)((n + 255) / 256 < 148 * 32 ? (n + 255) / 256 : 148 * 32);
   if (blocks < 1) blocks = 1;
   switch (vt) {
-    case ESB_VOXEL_F32: k_convert<ESB_VOXEL_F32><<<blocks, 256, 0, st>>>(vol, n, out, sign); break;
-    case ESB_VOXEL_F16: k_convert<ESB_VOXEL_F16><<<blocks, 256, 0, st>>>(vol, n, out, sign); break;
-    default: k_convert<ESB_VOXEL_BF16><<<blocks, 256, 0, st>>>(vol, n, out, sign); break;
+    case ESB_VOXEL_F32: k_convert<ESB_VOXEL_F32><<<blocks, 256, 0, st>>>(vol, n, out, sign); ESB_COUNT_LAUNCH(); break;
+    case ESB_VOXEL_F16: k_convert<ESB_VOXEL_F16><<<blocks, 256, 0, st>>>(vol, n, out, sign); ESB_COUNT_LAUNCH(); break;
+    default: k_convert<ESB_VOXEL_BF16><<<blocks, 256, 0, st>>>(vol, n, out, sign); ESB_COUNT_LAUNCH(); break;
   }
   return cudaGetLastError();
 }
@@ -409,9 +505,9 @@ cudaError_t launch_store(const float* in, long n, void* vol, int vt, cudaStream_
   int blocks = (int)((n + 255) / 256 < 148 * 32 ? (n + 255) / 256 : 148 * 32);
   if (blocks < 1) blocks = 1;
   switch (vt) {
-    case ESB_VOXEL_F32: k_store<ESB_VOXEL_F32><<<blocks, 256, 0, st>>>(in, n, vol); break;
-    case ESB_VOXEL_F16: k_store<ESB_VOXEL_F16><<<blocks, 256, 0, st>>>(in, n, vol); break;
-    default: k_store<ESB_VOXEL_BF16><<<blocks, 256, 0, st>>>(in, n, vol); break;
+    case ESB_VOXEL_F32: k_store<ESB_VOXEL_F32><<<blocks, 256, 0, st>>>(in, n, vol); ESB_COUNT_LAUNCH(); break;
+    case ESB_VOXEL_F16: k_store<ESB_VOXEL_F16><<<blocks, 256, 0, st>>>(in, n, vol); ESB_COUNT_LAUNCH(); break;
+    default: k_store<ESB_VOXEL_BF16><<<blocks, 256, 0, st>>>(in, n, vol); ESB_COUNT_LAUNCH(); break;
   }
   return cudaGetLastError();
 }

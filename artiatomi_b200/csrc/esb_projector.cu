@@ -319,9 +319,9 @@ cudaError_t launch_march(const KConst& c, const void* vol, int vt, float* proj, 
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
   dim3 blk(32, 8), grd((x1 - x0 + 31) / 32, (y1 - y0 + 7) / 8);
   switch (vt) {
-    case ESB_VOXEL_F32: k_march<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, x0, y0, x1, y1); break;
-    case ESB_VOXEL_F16: k_march<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, x0, y0, x1, y1); break;
-    default: k_march<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, x0, y0, x1, y1); break;
+    case ESB_VOXEL_F32: k_march<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, x0, y0, x1, y1); ESB_COUNT_LAUNCH(); break;
+    case ESB_VOXEL_F16: k_march<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, x0, y0, x1, y1); ESB_COUNT_LAUNCH(); break;
+    default: k_march<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, x0, y0, x1, y1); ESB_COUNT_LAUNCH(); break;
   }
   return cudaGetLastError();
 }
@@ -331,9 +331,9 @@ cudaError_t launch_slicer(const KConst& c, const void* vol, int vt, float* proj,
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
   dim3 blk(32, 8), grd((x1 - x0 + 31) / 32, (y1 - y0 + 7) / 8);
   switch (vt) {
-    case ESB_VOXEL_F32: k_slicer<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, proj, pitchE, tmin, tmax, x0, y0, x1, y1); break;
-    case ESB_VOXEL_F16: k_slicer<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, proj, pitchE, tmin, tmax, x0, y0, x1, y1); break;
-    default: k_slicer<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, proj, pitchE, tmin, tmax, x0, y0, x1, y1); break;
+    case ESB_VOXEL_F32: k_slicer<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, proj, pitchE, tmin, tmax, x0, y0, x1, y1); ESB_COUNT_LAUNCH(); break;
+    case ESB_VOXEL_F16: k_slicer<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, proj, pitchE, tmin, tmax, x0, y0, x1, y1); ESB_COUNT_LAUNCH(); break;
+    default: k_slicer<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, proj, pitchE, tmin, tmax, x0, y0, x1, y1); ESB_COUNT_LAUNCH(); break;
   }
   return cudaGetLastError();
 }
@@ -342,7 +342,7 @@ cudaError_t launch_travlen(const KConst& c, float* dist, size_t pitchE, int x0, 
                            cudaStream_t st) {
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
   dim3 blk(32, 8), grd((x1 - x0 + 31) / 32, (y1 - y0 + 7) / 8);
-  k_travlen<<<grd, blk, 0, st>>>(c, dist, pitchE, x0, y0, x1, y1);
+  k_travlen<<<grd, blk, 0, st>>>(c, dist, pitchE, x0, y0, x1, y1); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -353,9 +353,9 @@ cudaError_t launch_bp(const KConst& c, void* vol, int vt, const float* img, int 
   const float inv = 1.0f / (float)os;
   dim3 blk(32, 4, 1), grd((nq + 31) / 32, (ny + 3) / 4, nz);
   switch (vt) {
-    case ESB_VOXEL_F32: k_bp<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, img, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); break;
-    case ESB_VOXEL_F16: k_bp<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, img, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); break;
-    default: k_bp<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, img, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); break;
+    case ESB_VOXEL_F32: k_bp<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, img, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); ESB_COUNT_LAUNCH(); break;
+    case ESB_VOXEL_F16: k_bp<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, img, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); ESB_COUNT_LAUNCH(); break;
+    default: k_bp<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, img, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear); ESB_COUNT_LAUNCH(); break;
   }
   return cudaGetLastError();
 }

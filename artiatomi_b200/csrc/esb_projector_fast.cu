@@ -453,6 +453,7 @@ cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float*
     k_slicer_fused<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
   else
     k_slicer_fused<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
+  ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
@@ -461,8 +462,11 @@ cudaError_t launch_project_fast(const KConst& c, const void* vol, int vt, int mo
                                 cudaStream_t st) {
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
   dim3 blk(256), grd((x1 - x0 + 7) / 8, (y1 - y0 + 7) / 8);
-#define ESB_LAUNCH(VT, M) \
-  k_project_fast<VT, M><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, tmin, tmax, x0, y0, x1, y1)
+#define ESB_LAUNCH(VT, M)                                                                            \
+  do {                                                                                               \
+    k_project_fast<VT, M><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, tmin, tmax, x0, y0, x1, y1); \
+    ESB_COUNT_LAUNCH();                                                                              \
+  } while (0)
   if (mode == 0) {
     if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, 0);
     else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, 0);

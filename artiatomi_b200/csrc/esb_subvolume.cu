@@ -46,7 +46,7 @@ struct PairConst {
   int active;
 };
 
-__global__ void __launch_bounds__(kQuadsPerItem) k_subvol_batch(const SubvolWork* __restrict__ work, int n_work,
+__global__ void __launch_bounds__(kQuadsPerItem, 6) k_subvol_batch(const SubvolWork* __restrict__ work, int n_work,
                                                                 const SubvolParticle* __restrict__ parts,
                                                                 const PairConst* __restrict__ pairs, int n_list,
                                                                 int t0, int nt, const float* __restrict__ imgs,
@@ -169,7 +169,7 @@ cudaError_t subvol_batch_launch(const SubvolBatch& b, int t0, int nt, const floa
   k_subvol_batch<<<(unsigned)blocks, kQuadsPerItem, 0, st>>>(
       (const SubvolWork*)base, b.n_work, (const SubvolParticle*)(base + b.off_parts),
       (const PairConst*)(base + b.off_pairs), b.n_list, t0, nt, imgs, img_stride, slabs, pw, ph, os, 1.0f / (float)os,
-      linear);
+      linear); ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 

@@ -275,6 +275,11 @@ def device_view(address: int, shape, typestr: str = "<f4"):
     return torch.as_tensor(_CudaArray(address, shape, typestr), device="cuda")
 
 
+def kernel_launches() -> int:
+    """Kernel launches issued by the library so far in this process."""
+    return int(lib.esb_kernel_launches())
+
+
 # --------------------------------------------------------------------------- reconstructor
 @dataclass
 class ReconConfig:

@@ -2,12 +2,14 @@
 
   python -m artiatomi_b200.kernel_bench --kernel fp|slicer|bp|bp_linear
       [--dims X Y Z] [--proj W H] [--tilt DEG] [--os N] [--voxel f32|f16|bf16]
-      [--reps R] [--warmup N]
+      [--reps R] [--warmup N] [--fast]
 
 Prints one JSON line per kernel: mean ms per launch and algorithmic GB/s
 (forward projection: volume read once + projection/ray-length writes;
 back-projection: volume read + write + projection read). The volume is
-random; the geometry is one tilt of a single-axis series.
+random; the geometry is one tilt of a single-axis series. --fast times the
+closed-form projector / per-voxel-shadow back-projector instead of the
+faithful kernels.
 """
 from __future__ import annotations
 
@@ -32,6 +34,7 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--slab", type=float, default=111.1, help="slab thickness in voxels (slicer, bp slabs)")
+    ap.add_argument("--fast", action="store_true")
     a = ap.parse_args(argv)
     nx, ny, nz = a.dims
     W, H = a.proj if a.proj else (ny, nx)
@@ -51,15 +54,15 @@ def main(argv=None):
 
     def launch():
         if a.kernel == "fp":
-            E.forward_project(fc, vol, proj, dist)
+            E.forward_project(fc, vol, proj, dist, fast=a.fast)
         elif a.kernel == "slicer":
-            E.forward_project_slab(fc, vol, proj, mid - 0.5 * a.slab, mid + 0.5 * a.slab)
+            E.forward_project_slab(fc, vol, proj, mid - 0.5 * a.slab, mid + 0.5 * a.slab, fast=a.fast)
         elif a.kernel == "travlen":
             E.traversal_length(fc, dist)
         elif a.kernel == "bp":
-            E.back_project(bc, vol, img, 1e-3, a.os)
+            E.back_project(bc, vol, img, 1e-3, a.os, fast=a.fast)
         else:
-            E.back_project(bc, vol, img, 1e-3, a.os, mid - 0.5 * a.slab, mid + 0.5 * a.slab, True)
+            E.back_project(bc, vol, img, 1e-3, a.os, mid - 0.5 * a.slab, mid + 0.5 * a.slab, True, fast=a.fast)
 
     for _ in range(a.warmup):
         launch()
@@ -85,7 +88,7 @@ def main(argv=None):
         frac = min(1.0, a.slab / max(t1 - t0, 1e-6))
         nbytes = 2 * V * s * frac + P * 4
     mean = float(np.mean(ms))
-    print(json.dumps({"kernel": a.kernel, "dims": a.dims, "proj": [W, H], "tilt": a.tilt, "os": a.os,
+    print(json.dumps({"kernel": a.kernel, "fast": a.fast, "dims": a.dims, "proj": [W, H], "tilt": a.tilt, "os": a.os,
                       "voxel": a.voxel, "ms_mean": mean, "ms_min": float(np.min(ms)),
                       "algorithmic_GBps": nbytes / (mean * 1e-3) / 1e9}), flush=True)
 

@@ -11,16 +11,19 @@ tomogram frame, cubic boxes of 48/64/96 voxels in a 50/35/15 split, 61 tilts
 projections are synthetic: random ellipses with the line-integral profile of
 an ellipsoid plus Gaussian noise, made on the GPU.
 
-Both paths run through esb_subvolume_wbp of the FAST variant: batched = 0
-launches the back-projection once per particle per tilt (the reference's
-scheme), batched = 1 runs one persistent launch over all particles (per tilt
-with CTF, over all tilts without). Prints one JSON line with both timings
+Both paths run through esb_subvolume_wbp: batched = 1 (FAST variant) runs
+one persistent launch over all particles (per tilt with CTF, over all tilts
+without); batched = 0 launches the back-projection once per particle per
+tilt, with the FAST kernel (all slabs of a tilt in one launch, --plain fast)
+or, as the reference does, with the FAITHFUL kernel once per particle per
+slab (--plain faithful). Prints one JSON line with both timings
 (CUDA events around the whole call, and the back-projection phase alone),
 the speed-up and the relative L2 difference of the two results.
 """
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import time
 
@@ -99,6 +102,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--plain", choices=["fast", "faithful"], default="fast")
     a = ap.parse_args(argv)
     W = H = a.proj
     t_build = time.time()
@@ -106,6 +110,9 @@ def main(argv=None):
     projs = synthetic_projections(a.n_proj, W, H, a.seed + 1)
     il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, w["tilt"])
     rec = E.Reconstructor(w["cfg"], w["pg"], w["tilt"], w["defocus"])
+    plain_cfg = dataclasses.replace(w["cfg"], variant=E.VARIANT_FAST if a.plain == "fast" else E.VARIANT_FAITHFUL)
+    rec_plain = E.Reconstructor(plain_cfg, w["pg"], w["tilt"], w["defocus"])
+    recs = {False: rec_plain, True: rec}
     boxes = {b: [torch.zeros((int(s),) * 3, dtype=torch.float32, device="cuda") for s in w["sizes"]]
              for b in (False, True)}
     torch.cuda.synchronize()
@@ -117,7 +124,7 @@ def main(argv=None):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        rec.subvolume_wbp(w["full"], w["sub"], w["pair"], boxes[batched], projs, il, batched=batched)
+        recs[batched].subvolume_wbp(w["full"], w["sub"], w["pair"], boxes[batched], projs, il, batched=batched)
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
@@ -129,26 +136,27 @@ def main(argv=None):
         ms = [run(batched) for _ in range(a.reps)]
         # phase breakdown from one more run with per-launch events (kept out
         # of the timed runs: they add host work per launch)
-        rec.enable_timing(True)
-        rec.timing()
+        recs[batched].enable_timing(True)
+        recs[batched].timing()
         run(batched)
-        ph = rec.timing()
-        rec.enable_timing(False)
+        ph = recs[batched].timing()
+        recs[batched].enable_timing(False)
         res[batched] = dict(ms=float(np.median(ms)), bp_ms=ph["bp"][0], bp_launches=ph["bp"][1], ctf_ms=ph["ctf"][0])
     num = sum(float(((x - y).double() ** 2).sum()) for x, y in zip(boxes[True], boxes[False]))
     den = sum(float((y.double() ** 2).sum()) for y in boxes[False])
     voxels = int(sum(int(s) ** 3 for s in w["sizes"]))
     updates = voxels * len(il)
     rec.close()
+    rec_plain.close()
     print(json.dumps({
         "workload": "subvolume_wbp", "particles": a.particles, "frame": a.frame, "proj": [W, H],
-        "n_proj": a.n_proj, "oversampling": a.os, "ctf": not a.no_ctf, "voxels": voxels,
+        "n_proj": a.n_proj, "oversampling": a.os, "ctf": not a.no_ctf, "voxels": voxels, "plain": a.plain,
         "plain_ms": res[False]["ms"], "batched_ms": res[True]["ms"],
         "speedup": res[False]["ms"] / res[True]["ms"],
         "plain_bp_ms": res[False]["bp_ms"], "batched_bp_ms": res[True]["bp_ms"],
         "bp_speedup": res[False]["bp_ms"] / max(res[True]["bp_ms"], 1e-9),
         "plain_bp_launches": res[False]["bp_launches"], "batched_bp_launches": res[True]["bp_launches"],
-        "ctf_ms": res[True]["ctf_ms"],
+        "plain_ctf_ms": res[False]["ctf_ms"], "batched_ctf_ms": res[True]["ctf_ms"],
         "batched_voxel_updates_per_s": updates / (res[True]["ms"] * 1e-3),
         "rel_l2_batched_vs_plain": float(np.sqrt(num / max(den, 1e-300))),
         "setup_s": round(t_build, 1),

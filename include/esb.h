@@ -99,6 +99,10 @@ typedef struct esb_vol_geom {
 
 const char* esb_last_error(void);
 int esb_version(void);
+/* Number of kernel launches this library has issued in the process (all
+ * threads; cuFFT's own kernels not included). No counterpart in the
+ * reference: a diagnostic for launch-count claims. */
+unsigned long long esb_kernel_launches(void);
 
 /* ---------------------------------------------------------------- geometry
  * Host functions; no device work. */

@@ -52,3 +52,23 @@ def test_reconstructor_rejects_bad_config():
     cfg = E.ReconConfig(proj_x=8, proj_y=8, n_proj=1, ctf_mode=True)
     with pytest.raises(L.EsbError):
         E.Reconstructor(cfg, geoms, [0.0], stream=0)
+
+
+def test_kernel_launch_counter_starts_without_gpu_work():
+    assert E.kernel_launches() >= 0
+
+
+@pytest.mark.gpu
+def test_kernel_launch_counter_counts_launches():
+    from tests.helpers import cuda, small_case
+
+    case = small_case()
+    W, H = case["W"], case["H"]
+    c = E.set_constant_values(case["pg"][0], case["vg"])
+    vol = cuda(case["vol"])
+    proj = cuda(np.zeros((H, W), np.float32))
+    dist = cuda(np.zeros((H, W), np.float32))
+    n0 = E.kernel_launches()
+    E.forward_project(c, vol, proj, dist)
+    E.forward_project(c, vol, proj, dist, fast=True)
+    assert E.kernel_launches() - n0 == 2
