@@ -46,7 +46,7 @@ struct PairConst {
   int active;
 };
 
-__global__ void __launch_bounds__(kQuadsPerItem, 6) k_subvol_batch(const SubvolWork* __restrict__ work, int n_work,
+__global__ void __launch_bounds__(kQuadsPerItem) k_subvol_batch(const SubvolWork* __restrict__ work, int n_work,
                                                                 const SubvolParticle* __restrict__ parts,
                                                                 const PairConst* __restrict__ pairs, int n_list,
                                                                 int t0, int nt, const float* __restrict__ imgs,
