@@ -39,6 +39,16 @@ METRIC = "SART voxel-updates/s (SART+3D-CTF iteration, 1024x1024x256, 61x1024^2)
 UNIT = "voxel-updates/s"
 
 
+# DRAM bytes per launch measured by ncu (dram__bytes_read.sum,
+# dram__bytes_write.sum) on the 1024x1024x64 volume / 1024^2 detector case,
+# per unit of the roofline: forward projection = k_slicer_fused + k_travlen,
+# back-projection = k_bp_fast. The volume part scales with the voxels, the
+# image part with the pixels.
+DRAM_V, DRAM_P = 1024 * 1024 * 64, 1024 * 1024
+DRAM_FP_READ, DRAM_FP_IMG = 268.74e6, 4.77e6 + 4.20e6
+DRAM_BP_READ, DRAM_BP_WRITE, DRAM_BP_IMG = 274.97e6 - 4.19e6, 207.27e6, 4.19e6
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -307,10 +317,12 @@ def run_esb(args):
     if bp_ms >= fp_ms:
         slabs = bp_n / nproj
         bytes_unit = 2 * V * 4 + slabs * P * 4
+        traffic = (DRAM_BP_READ + DRAM_BP_WRITE) / DRAM_V * V + DRAM_BP_IMG / DRAM_P * P
         name, t_unit, launches = "back-projection (all slab launches of one projection)", bp_ms / nproj, bp_n
     else:
         slabs = (fp_n / nproj) - 1
         bytes_unit = V * 4 + (2 * slabs + 2) * P * 4
+        traffic = DRAM_FP_READ / DRAM_V * V + DRAM_FP_IMG / DRAM_P * P
         name, t_unit, launches = "forward projection (slicer launches + traversal length of one projection)", \
             fp_ms / nproj, fp_n
     achieved = bytes_unit / (t_unit * 1e-3) / 1e9
@@ -336,7 +348,9 @@ def run_esb(args):
                 "gpu_launches": int(gpu_launches),
                 "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm,
                              "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
-                             "traffic": None, "algorithmic_bytes_per_unit": bytes_unit, "ms_per_unit": t_unit,
+                             "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + "
+                             "dram__bytes_write.sum per launch on the 1024x1024x64 case, volume part scaled by "
+                             "voxels, image part by pixels", "algorithmic_bytes_per_unit": bytes_unit, "ms_per_unit": t_unit,
                              "launches": launches},
                 "phases_ms_per_step": {k: v[0] for k, v in phases.items()},
                 "clocks": clk.summary(),
