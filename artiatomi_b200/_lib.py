@@ -85,6 +85,8 @@ _SIGS = {
     "esb_fp_fast": ([C.POINTER(Constants), P, I, I, I, P, P, SZ, I, I, I, I, P], I),
     "esb_fp_slicer_fast": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, F, I, I, I, I, P], I),
     "esb_bp_fast": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, I, F, F, I, P], I),
+    "esb_fp_adjoint": ([C.POINTER(Constants), P, I, I, P, SZ, F, F, P], I),
+    "esb_projection_loss_grad": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, F, P, P, P, P], I),
     "esb_make_square": ([I, I, SZ, P, I, P, I, I, I, I, P], I),
     "esb_ctf": ([P, I, F, F, F, I, I, F, P, F, F, F, F, P], I),
     "esb_wbp_weighting": ([P, I, F, I, P], I),

@@ -32,6 +32,7 @@ UNITS = [
     ("esb_projector_fast.cu", []),
     ("esb_backprojector_fast.cu", []),
     ("esb_subvolume.cu", []),
+    ("esb_adjoint.cu", []),
     ("esb_image.cu", ["--fmad=false"]),
     ("esb_api.cu", []),
     ("esb_noalloc.cu", []),

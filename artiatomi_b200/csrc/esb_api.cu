@@ -51,6 +51,10 @@ cudaError_t launch_square_to_image_batch(const float* sq, int count, int maxsize
 cudaError_t launch_ctf_slabs(const float* in, float* out, size_t out_stride, int n, const CtfConst& k,
                              const CtfSlabs& slabs_nm, float angle_deg, int applyForFP, int phaseFlip, float wiener,
                              float4 beta, cudaStream_t st);
+cudaError_t launch_fp_adjoint(const KConst& c, float* grad, const float* img, size_t pitchE, float sx, float sy, int w,
+                              int h, cudaStream_t st);
+cudaError_t launch_loss_grad(const KConst& c, const void* vol, int vt, const float* meas, size_t pitchE, float sx,
+                             float sy, float* grad, float* proj_out, double* out, int w, int h, cudaStream_t st);
 CtfConst make_ctf_const(int n, float cs_mm, float voltage_kv, float amp_contrast, float pixel_size_nm);
 cudaError_t launch_ctf(float* spec, int n, const CtfConst& k, float d0_nm, float d1_nm, float angle_deg, int applyForFP,
                        int phaseFlip, float wiener, float4 beta, cudaStream_t st);
@@ -236,6 +240,30 @@ int esb_bp_fast(const esb_constants* c, void* vol, int voxel_type, int proj_x, i
     return fail(ESB_ERR_INVALID_ARGUMENT, "esb_bp_fast: volume_dim_x_quarter exceeds volume_dim.x / 4");
   ESB_CK(launch_bp_fast(to_kconst(*c), vol, voxel_type, img, proj_x, proj_y, pitch / 4, lambda, oversampling, dist_min,
                         dist_max, linear_filter, as_stream(stream)), "esb_bp_fast");
+  return ok();
+}
+
+int esb_fp_adjoint(const esb_constants* c, float* grad_vol, int proj_x, int proj_y, const float* img, size_t pitch,
+                   float shift_u, float shift_v, void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_fp_adjoint")) || (r = check_image(proj_x, proj_y, pitch, "esb_fp_adjoint"))) return r;
+  if (!grad_vol || !img) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_fp_adjoint: NULL argument");
+  ESB_CK(launch_fp_adjoint(to_kconst(*c), grad_vol, img, pitch / 4, shift_u, shift_v, proj_x, proj_y, as_stream(stream)),
+         "esb_fp_adjoint");
+  return ok();
+}
+
+int esb_projection_loss_grad(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y,
+                             const float* measured, size_t pitch, float shift_u, float shift_v, float* grad_vol,
+                             float* proj_out, double* out6, void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_projection_loss_grad")) ||
+      (r = check_image(proj_x, proj_y, pitch, "esb_projection_loss_grad")))
+    return r;
+  if (!vol || !out6 || !valid_vt(voxel_type))
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_projection_loss_grad: invalid argument");
+  ESB_CK(launch_loss_grad(to_kconst(*c), vol, voxel_type, measured, pitch / 4, shift_u, shift_v, grad_vol, proj_out,
+                          out6, proj_x, proj_y, as_stream(stream)), "esb_projection_loss_grad");
   return ok();
 }
 

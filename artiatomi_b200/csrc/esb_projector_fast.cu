@@ -24,68 +24,13 @@
 // are combined with warp shuffles.
 #include <float.h>
 
-#include "esb_device.cuh"
+#include "esb_ray_core.cuh"
 
 namespace esb {
 
 namespace {
 
-// Number of samples J of the float recurrence t_{j+1} = fl(t_j + h) from t0
-// with t_j <= tout, and its constant step; ok = false when the recurrence is
-// not an arithmetic progression over [t0, tout].
-__device__ __forceinline__ int progression(float t0, float tout, float h, float& step, bool& ok) {
-  ok = true;
-  step = h;
-  if (!(t0 <= tout)) return 0;
-  float t1 = __fadd_rn(t0, h);
-  step = __fsub_rn(t1, t0);
-  float t2 = __fadd_rn(t1, h);
-  if (!(t0 > 0.0f) || __fsub_rn(t2, t1) != step || !(step > 0.0f)) {
-    ok = false;
-    return 0;
-  }
-  int J = (int)__fdiv_rn(__fsub_rn(tout, t0), step) + 1;
-  if (J < 1) J = 1;
-  while (J > 1 && __fadd_rn(t0, __fmul_rn((float)(J - 1), step)) > tout) --J;
-  while (__fadd_rn(t0, __fmul_rn((float)J, step)) <= tout) ++J;
-  // the last sample must stay in the binade of t0 (exact arithmetic there)
-  const float tl = __fadd_rn(t0, __fmul_rn((float)(J - 1), step));
-  int e0, e1;
-  frexpf(t0, &e0);
-  frexpf(tl, &e1);
-  if (e0 != e1) ok = false;
-  return J;
-}
-
-template <int VT>
-struct Cell {
-  const void* __restrict__ vol;
-  int nx, ny, nz;
-  long sy, sz;
-  __device__ __forceinline__ float at(int x, int y, int z) const {
-    x = x < 0 ? 0 : (x > nx - 1 ? nx - 1 : x);
-    y = y < 0 ? 0 : (y > ny - 1 ? ny - 1 : y);
-    z = z < 0 ? 0 : (z > nz - 1 ? nz - 1 : z);
-    return Voxel<VT>::load(vol, (long)z * sz + (long)y * sy + x);
-  }
-};
-
-// Trilinear sample at interpolation coordinates (x, y, z) (texel centres at
-// integers), clamp addressing.
-template <int VT>
-__device__ __forceinline__ float trilinear(const Cell<VT>& C, float x, float y, float z) {
-  float fx = floorf(x), fy = floorf(y), fz = floorf(z);
-  float a = x - fx, b = y - fy, c = z - fz;
-  int ix = (int)fmaxf(fminf(fx, 1.0e9f), -1.0e9f), iy = (int)fmaxf(fminf(fy, 1.0e9f), -1.0e9f),
-      iz = (int)fmaxf(fminf(fz, 1.0e9f), -1.0e9f);
-  float c000 = C.at(ix, iy, iz), c100 = C.at(ix + 1, iy, iz), c010 = C.at(ix, iy + 1, iz),
-        c110 = C.at(ix + 1, iy + 1, iz);
-  float c001 = C.at(ix, iy, iz + 1), c101 = C.at(ix + 1, iy, iz + 1), c011 = C.at(ix, iy + 1, iz + 1),
-        c111 = C.at(ix + 1, iy + 1, iz + 1);
-  float ia = 1.f - a, ib = 1.f - b, ic = 1.f - c;
-  return ic * (ib * (ia * c000 + a * c100) + b * (ia * c010 + a * c110)) +
-         c * (ib * (ia * c001 + a * c101) + b * (ia * c011 + a * c111));
-}
+using namespace raycore;
 
 // Sum of the trilinear interpolant over samples j = j0 .. J-1 at coordinates
 // q + j*dq, by exact cell-wise closed forms.
@@ -94,7 +39,7 @@ __device__ float cell_sum(const Cell<VT>& C, float qx, float qy, float qz, float
                           int J) {
   if (j0 >= J) return 0.0f;
   // position of sample j0
-  float px = qx + (float)j0 * dqx, py = qy + (float)j0 * dqy, pz = qz + (float)j0 * dqz;
+  float px = qpos(qx, j0, dqx), py = qpos(qy, j0, dqy), pz = qpos(qz, j0, dqz);
   float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
   int ix = (int)fx, iy = (int)fy, iz = (int)fz;
   // sample parameter s (in units of j, relative to j0) of the next boundary per axis
@@ -121,9 +66,9 @@ __device__ float cell_sum(const Cell<VT>& C, float qx, float qy, float qz, float
     if (m1 > M_total) m1 = M_total;
     if (m1 > m0) {
       // local coordinates of sample m0 and per-sample increments
-      const float a0 = (qx + (float)(j0 + m0) * dqx) - (float)ix;
-      const float b0 = (qy + (float)(j0 + m0) * dqy) - (float)iy;
-      const float e0 = (qz + (float)(j0 + m0) * dqz) - (float)iz;
+      const float a0 = __fsub_rn(qpos(qx, j0 + m0, dqx), (float)ix);
+      const float b0 = __fsub_rn(qpos(qy, j0 + m0, dqy), (float)iy);
+      const float e0 = __fsub_rn(qpos(qz, j0 + m0, dqz), (float)iz);
       const float M = (float)(m1 - m0);
       const float S1 = 0.5f * M * (M - 1.f);
       const float S2 = S1 * (2.f * M - 1.f) * (1.f / 3.f);
@@ -193,7 +138,7 @@ template <int VT>
 __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float qz, float dqx, float dqz, int j0,
                              int J) {
   if (j0 >= J) return 0.0f;
-  const float px = qx + (float)j0 * dqx, pz = qz + (float)j0 * dqz;
+  const float px = qpos(qx, j0, dqx), pz = qpos(qz, j0, dqz);
   const float fx = floorf(px), fz = floorf(pz);
   int ix = (int)fx, iz = (int)fz;
   const float inf = FLT_MAX;
@@ -221,8 +166,8 @@ __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float
     int m1 = (sexit >= (float)M_total) ? M_total : (int)ceilf(sexit);
     if (m1 > M_total) m1 = M_total;
     if (m1 > m0) {
-      const float a0 = (qx + (float)(j0 + m0) * dqx) - (float)ix;
-      const float c0 = (qz + (float)(j0 + m0) * dqz) - (float)iz;
+      const float a0 = __fsub_rn(qpos(qx, j0 + m0, dqx), (float)ix);
+      const float c0 = __fsub_rn(qpos(qz, j0 + m0, dqz), (float)iz);
       const float M = (float)(m1 - m0);
       const float S1 = 0.5f * M * (M - 1.f);
       const float S2 = S1 * (2.f * M - 1.f) * (1.f / 3.f);
@@ -258,45 +203,6 @@ __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float
   return acc;
 }
 
-// Ray start and box entry/exit: the reference's expressions, operation by
-// operation without contraction, so t_in/t_out (|t| ~ 1e4) and hence the
-// sample positions and ray lengths equal the reference's FP32 values.
-__device__ __forceinline__ float mul_add_rn(float a, float b, float c) { return __fadd_rn(__fmul_rn(a, b), c); }
-
-__device__ __forceinline__ float3 ray_src(const KConst& c, float px, float py) {
-  float xA = __fadd_rn(__fadd_rn(__fmul_rn(c.aniso[0], px), __fmul_rn(c.aniso[1], py)), __fmul_rn(c.aniso[2], 1.0f));
-  float yA = __fadd_rn(__fadd_rn(__fmul_rn(c.aniso[3], px), __fmul_rn(c.aniso[4], py)), __fmul_rn(c.aniso[5], 1.0f));
-  float3 s;
-  s.x = mul_add_rn(yA, c.v.x, mul_add_rn(xA, c.u.x, c.det.x));
-  s.y = mul_add_rn(yA, c.v.y, mul_add_rn(xA, c.u.y, c.det.y));
-  s.z = mul_add_rn(yA, c.v.z, mul_add_rn(xA, c.u.z, c.det.z));
-  return s;
-}
-
-__device__ __forceinline__ void hit(float3 s, float3 d, float3 lo, float3 hi, float& tin, float& tout) {
-  float ex = __fdiv_rn(__fsub_rn(lo.x, s.x), d.x), ey = __fdiv_rn(__fsub_rn(lo.y, s.y), d.y),
-        ez = __fdiv_rn(__fsub_rn(lo.z, s.z), d.z);
-  float xx = __fdiv_rn(__fsub_rn(hi.x, s.x), d.x), xy = __fdiv_rn(__fsub_rn(hi.y, s.y), d.y),
-        xz = __fdiv_rn(__fsub_rn(hi.z, s.z), d.z);
-  tin = fmaxf(fmaxf(fminf(ex, xx), fminf(ey, xy)), fminf(ez, xz));
-  tout = fminf(fminf(fmaxf(ex, xx), fmaxf(ey, xy)), fmaxf(ez, xz));
-}
-
-// Sum of the 4 sub-ray values of a pixel (adjacent lanes) in the reference's
-// order ((v0 + v1) + v2) + v3, valid in the group's first lane.
-__device__ __forceinline__ float quad_sum_ordered(float v) {
-  const float v1 = __shfl_down_sync(0xffffffffu, v, 1);
-  const float v2 = __shfl_down_sync(0xffffffffu, v, 2);
-  const float v3 = __shfl_down_sync(0xffffffffu, v, 3);
-  return __fadd_rn(__fadd_rn(__fadd_rn(v, v1), v2), v3);
-}
-
-// Interpolation coordinates (texel centres at integers) of world point p.
-__device__ __forceinline__ float3 interp_coord(const KConst& c, float3 p) {
-  return make_float3((p.x - c.bbMin.x) * c.bbRcp.x * c.dim.x - 0.5f, (p.y - c.bbMin.y) * c.bbRcp.y * c.dim.y - 0.5f,
-                     (p.z - c.bbMin.z) * c.bbRcp.z * c.dim.z - c.zShift - 0.5f);
-}
-
 // Sum over the samples of one sub-ray from t0 to tout (first_at_source: the
 // slicer's first sample is taken at the ray start, ForwardProjectionSlicer.cu:126-141).
 template <int VT>
@@ -311,7 +217,7 @@ __device__ float ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0,
     bool first = true;
 #pragma unroll 1
     while (t <= tout) {
-      float3 p = first && first_at_source ? s : make_float3(s.x + t * c.n.x, s.y + t * c.n.y, s.z + t * c.n.z);
+      float3 p = first && first_at_source ? s : ray_point(c, s, t);
       float3 q = interp_coord(c, p);
       sum += trilinear<VT>(C, q.x, q.y, q.z);
       first = false;
@@ -320,9 +226,9 @@ __device__ float ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0,
     return sum;
   }
   // q(j) = q(t0) + j * dq
-  float3 q0 = interp_coord(c, make_float3(s.x + t0 * c.n.x, s.y + t0 * c.n.y, s.z + t0 * c.n.z));
-  const float dqx = step * c.n.x * c.bbRcp.x * c.dim.x, dqy = step * c.n.y * c.bbRcp.y * c.dim.y,
-              dqz = step * c.n.z * c.bbRcp.z * c.dim.z;
+  float3 q0 = interp_coord(c, ray_point(c, s, t0));
+  const float3 dq = interp_step(c, step);
+  const float dqx = dq.x, dqy = dq.y, dqz = dq.z;
   float sum = 0.0f;
   int j0 = 0;
   if (first_at_source) {
@@ -331,7 +237,7 @@ __device__ float ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0,
     j0 = 1;
   }
   // y stays in one cell and moves by < 1e-5 voxel over the ray: bilinear x-z walk
-  const float ylast = q0.y + (float)(J - 1) * dqy;
+  const float ylast = qpos(q0.y, J - 1, dqy);
   if (fabsf(dqy) * (float)J < 1e-5f && floorf(q0.y) == floorf(ylast)) {
     const float fy = floorf(q0.y);
     return sum + cell_sum_xz<VT>(C, q0.x, q0.y - fy, (int)fy, q0.z, dqx, dqz, j0, J);

@@ -207,6 +207,31 @@ def back_project(c: L.Constants, vol, img, lam: float, oversampling: int = 1, di
                      dist_max, int(linear), _stream(stream)))
 
 
+def fp_adjoint(c: L.Constants, grad, img, shift=(0.0, 0.0), stream=None) -> None:
+    """grad += A^T img, the transpose of forward_project(..., fast=True)'s
+    projection with detector offset `shift` (pixels). grad: FP32 volume."""
+    w, h, pitch = _img_args(img)
+    check(lib.esb_fp_adjoint(C.byref(c), fptr(grad), w, h, fptr(img), pitch, float(shift[0]), float(shift[1]),
+                             _stream(stream)))
+
+
+def projection_loss_grad(c: L.Constants, vol, measured, out, shift=(0.0, 0.0), grad=None, proj_out=None,
+                         width: int | None = None, height: int | None = None, stream=None) -> None:
+    """One tilt of L = 1/2 ||A(x, shift) - measured||^2. Adds to `out` (6
+    float64 on the device): L, dL/dshift_u, dL/dshift_v and the Gauss-Newton
+    terms sum (dp/du)^2, sum dp/du dp/dv, sum (dp/dv)^2; grad (FP32 volume,
+    optional) += dL/dx; proj_out (optional) = A(x, shift). measured may be
+    None (taken as 0), then width/height give the image size."""
+    ref = measured if measured is not None else proj_out
+    if ref is not None:
+        w, h, pitch = _img_args(ref)
+    else:
+        w, h, pitch = int(width), int(height), int(width) * 4
+    check(lib.esb_projection_loss_grad(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(measured), pitch,
+                                       float(shift[0]), float(shift[1]), fptr(grad), fptr(proj_out), fptr(out),
+                                       _stream(stream)))
+
+
 def make_square(img, maxsize: int, out, border_x: int, border_y: int, mirror_y=False, fill_zero=True, stream=None):
     w, h, pitch = _img_args(img)
     check(lib.esb_make_square(w, h, pitch, fptr(img), maxsize, fptr(out), border_x, border_y, int(mirror_y),

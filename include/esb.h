@@ -210,6 +210,32 @@ int esb_bp_fast(const esb_constants* c, void* vol, int voxel_type, int proj_x, i
                 size_t pitch, float lambda, int oversampling, float dist_min, float dist_max, int linear_filter,
                 void* stream);
 
+/* ------------------------------------------------------- differentiation
+ * No counterpart in the reference (its shift search, EmSartRefine.cpp:707-1100,
+ * cross-correlates projections instead). The model is esb_fp_fast's
+ * projection (march mode, `proj` only) with a detector offset (shift_u,
+ * shift_v) in pixels, applied as a rigid in-plane translation of every
+ * sample by shift_u * u + shift_v * v (the detector's pixel axes through the
+ * magnification anisotropy); each ray keeps the unshifted sample set, so the
+ * model is smooth in the offset. With zero offset it equals esb_fp_fast. */
+
+/* grad_vol += A^T img: the exact transpose of that projection (atomic adds,
+ * FP32 volume; zero grad_vol first for A^T img alone). */
+int esb_fp_adjoint(const esb_constants* c, float* grad_vol, int proj_x, int proj_y, const float* img, size_t pitch,
+                   float shift_u, float shift_v, void* stream);
+
+/* One tilt of L = 1/2 sum (A(x, s) - measured)^2, with per-ray
+ * recomputation (nothing stored per ray). Adds to out6 (device, 6 doubles):
+ * [0] L, [1] dL/dshift_u, [2] dL/dshift_v, and the Gauss-Newton terms
+ * [3] sum (dp/dshift_u)^2, [4] sum dp/dshift_u * dp/dshift_v,
+ * [5] sum (dp/dshift_v)^2. grad_vol (FP32, may be NULL) += dL/dx.
+ * proj_out (may be NULL) = A(x, s). measured may be NULL (taken as 0). For
+ * a sub-volume, pass the particle box's constants: the offsets are then
+ * per particle and tilt. */
+int esb_projection_loss_grad(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y,
+                             const float* measured, size_t pitch, float shift_u, float shift_v, float* grad_vol,
+                             float* proj_out, double* out6, void* stream);
+
 /* CopyToSquareKernel::operator() (Kernels.cpp:808-850) -> `makeSquare`
  * (CopyToSquare.cu:38-92); out is dense maxsize x maxsize. */
 int esb_make_square(int proj_x, int proj_y, size_t pitch, const float* in, int maxsize, float* out, int border_x,

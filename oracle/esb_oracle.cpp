@@ -878,3 +878,221 @@ int orc_float_to_bf16(const float* in, uint16_t* out, long n) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------ differentiable projection model
+// CPU counterpart of esb_projection_loss_grad / esb_fp_adjoint (the GPU
+// library's esb_adjoint.cu). The reference has no gradient; the model is the
+// fast projector's: each sub-ray sums the trilinear interpolant over the
+// samples of the reference's float ray recurrence, and a detector offset
+// (s_u, s_v) in pixels translates every sample rigidly by s_u * u + s_v * v
+// (pixel axes through the magnification anisotropy). This function places
+// the unshifted samples with the GPU's float operations (ray source, box
+// entry, step, first sample, per-sample step), adds the translation in
+// double and evaluates values, gradients, the loss and the adjoint scatter
+// in double, sample by sample.
+namespace {
+
+struct ModelOut {
+  double part[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<double> grad;
+};
+
+// trilinear value and gradient (interpolation coordinates) at q, clamp
+// addressing; optional scatter of w * basis into g
+inline void model_sample(const VolView& V, double qx, double qy, double qz, double& val, double& ga, double& gb,
+                         double& gc, double* g, double w) {
+  const double fx = std::floor(qx), fy = std::floor(qy), fz = std::floor(qz);
+  const double a = qx - fx, b = qy - fy, c = qz - fz;
+  auto cl = [](double f, int n) -> long {
+    long i = (long)std::max(std::min(f, 1.0e9), -1.0e9);
+    return i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
+  };
+  const long x0 = cl(fx, V.nx), x1 = cl(fx + 1, V.nx), y0 = cl(fy, V.ny), y1 = cl(fy + 1, V.ny);
+  const long z0 = cl(fz, V.nz), z1 = cl(fz + 1, V.nz);
+  const long sy = V.nx, sz = (long)V.nx * V.ny;
+  const long idx[8] = {z0 * sz + y0 * sy + x0, z0 * sz + y0 * sy + x1, z0 * sz + y1 * sy + x0,
+                       z0 * sz + y1 * sy + x1, z1 * sz + y0 * sy + x0, z1 * sz + y0 * sy + x1,
+                       z1 * sz + y1 * sy + x0, z1 * sz + y1 * sy + x1};
+  double cv[8];
+  for (int k = 0; k < 8; ++k) cv[k] = V.at(idx[k]);
+  const double ia = 1 - a, ib = 1 - b, ic = 1 - c;
+  const double B[8] = {ia * ib * ic, a * ib * ic, ia * b * ic, a * b * ic, ia * ib * c, a * ib * c, ia * b * c, a * b * c};
+  val = 0;
+  for (int k = 0; k < 8; ++k) val += B[k] * cv[k];
+  ga = ib * ic * (cv[1] - cv[0]) + b * ic * (cv[3] - cv[2]) + ib * c * (cv[5] - cv[4]) + b * c * (cv[7] - cv[6]);
+  gb = ia * ic * (cv[2] - cv[0]) + a * ic * (cv[3] - cv[1]) + ia * c * (cv[6] - cv[4]) + a * c * (cv[7] - cv[5]);
+  gc = ia * ib * (cv[4] - cv[0]) + a * ib * (cv[5] - cv[1]) + ia * b * (cv[6] - cv[2]) + a * b * (cv[7] - cv[3]);
+  if (g)
+    for (int k = 0; k < 8; ++k) g[idx[k]] += w * B[k];
+}
+
+// float operations of the GPU model
+struct ModelRayGeom {
+  float s[3];
+  float tin, tout;
+};
+
+inline void model_ray_geom(const OrcGeom& G, float px, float py, ModelRayGeom& R) {
+  const float xA = (G.aniso[0] * px + G.aniso[1] * py) + G.aniso[2] * 1.0f;
+  const float yA = (G.aniso[3] * px + G.aniso[4] * py) + G.aniso[5] * 1.0f;
+  for (int k = 0; k < 3; ++k) R.s[k] = yA * G.v[k] + (xA * G.u[k] + G.det[k]);
+  float lo[3], hi[3];
+  for (int k = 0; k < 3; ++k) {
+    const float e = (G.bbMin[k] - R.s[k]) / G.n[k], x = (G.bbMax[k] - R.s[k]) / G.n[k];
+    lo[k] = std::fmin(e, x);
+    hi[k] = std::fmax(e, x);
+  }
+  R.tin = std::fmax(std::fmax(lo[0], lo[1]), lo[2]);
+  R.tout = std::fmin(std::fmin(hi[0], hi[1]), hi[2]);
+}
+
+inline float model_interp(const OrcGeom& G, int k, float p) {
+  float q = ((p - G.bbMin[k]) * G.bbRcp[k]) * G.dim[k];
+  if (k == 2) q = q - G.zShift;
+  return q - 0.5f;
+}
+
+inline int model_progression(float t0, float tout, float h, float& step, bool& ok) {
+  ok = true;
+  step = h;
+  if (!(t0 <= tout)) return 0;
+  const float t1 = t0 + h;
+  step = t1 - t0;
+  const float t2 = t1 + h;
+  if (!(t0 > 0.0f) || t2 - t1 != step || !(step > 0.0f)) {
+    ok = false;
+    return 0;
+  }
+  int J = (int)((tout - t0) / step) + 1;
+  if (J < 1) J = 1;
+  while (J > 1 && t0 + (float)(J - 1) * step > tout) --J;
+  while (t0 + (float)J * step <= tout) ++J;
+  const float tl = t0 + (float)(J - 1) * step;
+  int e0, e1;
+  std::frexp(t0, &e0);
+  std::frexp(tl, &e1);
+  if (e0 != e1) ok = false;
+  return J;
+}
+
+// one sub-ray: sum of values and of gradients; with g != nullptr, scatter w
+void model_subray(const OrcGeom& G, const VolView& V, const ModelRayGeom& R, const double* d, double& sum, double& ga,
+                  double& gb, double& gc, double* g, double w) {
+  sum = ga = gb = gc = 0;
+  const float h = G.vs[0] * 0.15f;
+  float step;
+  bool ok;
+  const int J = model_progression(R.tin, R.tout, h, step, ok);
+  if (!(R.tin <= R.tout)) return;
+  auto acc = [&](double qx, double qy, double qz) {
+    double v, a, b, c;
+    model_sample(V, qx, qy, qz, v, a, b, c, g, w);
+    sum += v;
+    ga += a;
+    gb += b;
+    gc += c;
+  };
+  if (!ok) {
+    float t = R.tin;
+    for (int guard = 0; guard < (1 << 22) && t <= R.tout; ++guard) {
+      float q[3];
+      for (int k = 0; k < 3; ++k) q[k] = model_interp(G, k, std::fmaf(t, G.n[k], R.s[k]));
+      acc(q[0] + d[0], q[1] + d[1], q[2] + d[2]);
+      t += h;
+    }
+    return;
+  }
+  float q0[3], dq[3];
+  for (int k = 0; k < 3; ++k) {
+    q0[k] = model_interp(G, k, std::fmaf(R.tin, G.n[k], R.s[k]));
+    dq[k] = ((step * G.n[k]) * G.bbRcp[k]) * G.dim[k];
+  }
+  // the GPU rounds the translated first sample to float; the flat-y test
+  // is taken on that value
+  const float q0y = q0[1] + (float)d[1];
+  const float ylast = std::fmaf((float)(J - 1), dq[1], q0y);
+  const bool flat = std::fabs(dq[1]) * (float)J < 1e-5f && std::floor(q0y) == std::floor(ylast);
+  for (int j = 0; j < J; ++j)
+    acc((double)q0[0] + d[0] + j * (double)dq[0], (double)q0[1] + d[1] + (flat ? 0.0 : j * (double)dq[1]),
+        (double)q0[2] + d[2] + j * (double)dq[2]);
+}
+
+}  // namespace
+
+extern "C" {
+
+// out6 += [L, dL/ds_u, dL/ds_v, sum (dp/ds_u)^2, sum dp/ds_u dp/ds_v,
+// sum (dp/ds_v)^2]; grad_vol (double, may be NULL) += dL/dx; proj_out (may
+// be NULL) = A(x, s); meas may be NULL (0).
+int orc_model_loss_grad(const OrcGeom* g, const float* vol, int proj_x, int proj_y, const float* meas, float shift_u,
+                        float shift_v, double* grad_vol, float* proj_out, double* out6, int nthreads) {
+  const OrcGeom& G = *g;
+  VolView V{vol, (int)G.dim[0], (int)G.dim[1], (int)G.dim[2], 0};
+  const long nvox = (long)V.nx * V.ny * V.nz;
+  const double kappa = (double)(G.vs[0] * 0.15f * 0.25f);
+  // translation of the interpolation coordinates per pixel of offset
+  double tu[3], tv[3], d[3];
+  for (int k = 0; k < 3; ++k) {
+    const double S = (double)G.bbRcp[k] * G.dim[k];
+    tu[k] = ((double)G.aniso[0] * G.u[k] + (double)G.aniso[3] * G.v[k]) * S;
+    tv[k] = ((double)G.aniso[1] * G.u[k] + (double)G.aniso[4] * G.v[k]) * S;
+    d[k] = shift_u * tu[k] + shift_v * tv[k];
+  }
+  const int nt = std::max(1, std::min(nthreads, proj_y));
+  std::vector<ModelOut> outs(nt);
+  for (auto& o : outs)
+    if (grad_vol) o.grad.assign(nvox, 0.0);
+  std::atomic<int> next(0);
+  auto work = [&](int tid) {
+    ModelOut& O = outs[tid];
+    for (;;) {
+      const int y = next.fetch_add(1);
+      if (y >= proj_y) break;
+      for (int x = 0; x < proj_x; ++x) {
+        ModelRayGeom R[4];
+        double sum = 0, du = 0, dv = 0;
+        bool hitr[4];
+        for (int sub = 0; sub < 4; ++sub) {
+          const float osx = (sub & 2) ? 0.75f : 0.25f, osy = (sub & 1) ? 0.75f : 0.25f;
+          model_ray_geom(G, (float)x + osx, (float)y + osy, R[sub]);
+          hitr[sub] = R[sub].tout - R[sub].tin > 0.0f;
+          if (!hitr[sub]) continue;
+          double s, a, b, c;
+          model_subray(G, V, R[sub], d, s, a, b, c, nullptr, 0.0);
+          du += a * tu[0] + b * tu[1] + c * tu[2];
+          dv += a * tv[0] + b * tv[1] + c * tv[2];
+          sum += s;
+        }
+        const double p = kappa * sum;
+        const size_t i = (size_t)y * proj_x + x;
+        if (proj_out) proj_out[i] = (float)p;
+        const double r = meas ? p - (double)meas[i] : p;
+        du *= kappa;
+        dv *= kappa;
+        O.part[0] += 0.5 * r * r;
+        O.part[1] += r * du;
+        O.part[2] += r * dv;
+        O.part[3] += du * du;
+        O.part[4] += du * dv;
+        O.part[5] += dv * dv;
+        if (grad_vol && r != 0.0)
+          for (int sub = 0; sub < 4; ++sub) {
+            if (!hitr[sub]) continue;
+            double s, a, b, c;
+            model_subray(G, V, R[sub], d, s, a, b, c, O.grad.data(), r * kappa);
+          }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t) pool.emplace_back(work, t);
+  for (auto& th : pool) th.join();
+  for (auto& o : outs) {
+    for (int q = 0; q < 6; ++q) out6[q] += o.part[q];
+    if (grad_vol)
+      for (long v = 0; v < nvox; ++v) grad_vol[v] += o.grad[v];
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -35,6 +35,7 @@ _SIGS = {
     "orc_float_to_half": [P, P, L],
     "orc_half_to_float": [P, P, L],
     "orc_float_to_bf16": [P, P, L],
+    "orc_model_loss_grad": [C.POINTER(OrcGeom), P, I, I, P, F, F, P, P, P, I],
 }
 
 
