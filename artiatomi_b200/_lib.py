@@ -101,6 +101,7 @@ _SIGS = {
     "esb_rec_reset_projections": ([P], I),
     "esb_reconstructor_enable_timing": ([P, I], I),
     "esb_reconstructor_timing": ([P, P, P], I),
+    "esb_reconstructor_enable_graphs": ([P, I], I),
     "esb_rec_forward_projection": ([P, C.POINTER(VolGeom), P, I, I, I], I),
     "esb_rec_compare": ([P, C.POINTER(VolGeom), P, I], I),
     "esb_rec_back_projection": ([P, C.POINTER(VolGeom), P, I, I, F], I),

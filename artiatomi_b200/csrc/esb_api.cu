@@ -76,6 +76,7 @@ int fail(int code, const std::string& msg) {
 }
 
 static int cuda_fail(cudaError_t e, const char* where) {
+  cudaGetLastError();  // a non-sticky error must not resurface in the next call
   return fail(ESB_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
@@ -386,6 +387,9 @@ struct esb_reconstructor {
   int batch_slabs = 0;
   cufftHandle c2r_many[ESB_CTF_SLAB_BATCH + 1] = {};
   bool c2r_many_ok[ESB_CTF_SLAB_BATCH + 1] = {};
+  bool graphs = false;                   // replay SART iterations from a captured graph
+  cudaGraphExec_t sart_exec = nullptr;   // the last captured iteration
+  cudaStream_t capture_stream = nullptr;  // private stream the capture records on
 };
 
 // Brackets a phase of launches with events when timing is enabled.
@@ -435,6 +439,15 @@ static void rec_free(esb_reconstructor* r) {
   r->slab_imgs = nullptr;
   r->slab_cap = 0;
   subvol_batch_free(r->batch);
+  if (r->sart_exec) {
+    cudaStreamSynchronize(r->stream);
+    cudaGraphExecDestroy(r->sart_exec);
+    r->sart_exec = nullptr;
+  }
+  if (r->capture_stream) {
+    cudaStreamDestroy(r->capture_stream);
+    r->capture_stream = nullptr;
+  }
   cudaFree(r->spec_batch);
   cudaFree(r->sq_batch);
   r->spec_batch = r->sq_batch = nullptr;
@@ -515,6 +528,12 @@ int esb_reconstructor_enable_timing(esb_reconstructor* rec, int enable) {
   if (!rec) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_enable_timing: NULL reconstructor");
   rec->timing = enable != 0;
   for (auto& t : rec->timers) t.used = 0;
+  return ok();
+}
+
+int esb_reconstructor_enable_graphs(esb_reconstructor* rec, int enable) {
+  if (!rec) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_enable_graphs: NULL reconstructor");
+  rec->graphs = enable != 0;
   return ok();
 }
 
@@ -866,6 +885,38 @@ int esb_rec_back_projection(esb_reconstructor* r, const esb_vol_geom* vg, void* 
   return rec_back_project_image(r, vg, vol, voxel_type, index, sirt_count, r->proj_d);
 }
 
+}  // extern "C"
+
+// One SART iteration of EmSart.cpp:579-675: ordered subsets of sirt_count
+// projections, {FP, compare} for each, then {BP} for each.
+static int sart_iteration(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type,
+                          const float* projections, const int* index_list, int proj_count, int sirt_count,
+                          int* volume_is_empty) {
+  const size_t img = (size_t)r->cfg.proj_x * r->cfg.proj_y;
+  int rc;
+  const int steps = (proj_count + sirt_count - 1) / sirt_count;
+  for (int s = 0; s < steps; ++s) {
+    for (int i = 0; i < sirt_count; ++i) {
+      if (s * sirt_count + i >= proj_count) continue;
+      const int index = index_list[s * sirt_count + i];
+      if ((rc = esb_rec_reset_projections(r))) return rc;
+      if ((rc = esb_rec_forward_projection(r, vg, vol, voxel_type, index, *volume_is_empty))) return rc;
+      if ((rc = esb_rec_compare(r, vg, projections + (size_t)index * img, index))) return rc;
+      ESB_CK(cudaMemcpyAsync(r->sirt_d[i], r->proj_d, img * sizeof(float), cudaMemcpyDeviceToDevice, r->stream),
+             "esb_sart_run");
+    }
+    for (int i = 0; i < sirt_count; ++i) {
+      if (s * sirt_count + i >= proj_count) continue;
+      *volume_is_empty = 0;
+      const int index = index_list[s * sirt_count + i];
+      if ((rc = rec_back_project_image(r, vg, vol, voxel_type, index, (float)sirt_count, r->sirt_d[i]))) return rc;
+    }
+  }
+  return ESB_OK;
+}
+
+extern "C" {
+
 int esb_sart_run(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type, const float* projections,
                  const int* index_list, int proj_count, int iterations, int sirt_count, int* volume_is_empty) {
   if (!r || !vg || !vol || !projections || !index_list || !volume_is_empty || !valid_vt(voxel_type))
@@ -883,26 +934,52 @@ int esb_sart_run(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int vo
     r->sirt_d.push_back(p);
   }
   int rc;
-  // EmSart.cpp:579-675
-  for (int iter = 0; iter < iterations; ++iter) {
-    const int steps = (proj_count + sirt_count - 1) / sirt_count;
-    for (int s = 0; s < steps; ++s) {
-      for (int i = 0; i < sirt_count; ++i) {
-        if (s * sirt_count + i >= proj_count) continue;
-        const int index = index_list[s * sirt_count + i];
-        if ((rc = esb_rec_reset_projections(r))) return rc;
-        if ((rc = esb_rec_forward_projection(r, vg, vol, voxel_type, index, *volume_is_empty))) return rc;
-        if ((rc = esb_rec_compare(r, vg, projections + (size_t)index * img, index))) return rc;
-        ESB_CK(cudaMemcpyAsync(r->sirt_d[i], r->proj_d, img * sizeof(float), cudaMemcpyDeviceToDevice, r->stream),
-               "esb_sart_run");
-      }
-      for (int i = 0; i < sirt_count; ++i) {
-        if (s * sirt_count + i >= proj_count) continue;
-        *volume_is_empty = 0;
-        const int index = index_list[s * sirt_count + i];
-        if ((rc = rec_back_project_image(r, vg, vol, voxel_type, index, (float)sirt_count, r->sirt_d[i]))) return rc;
-      }
+  int iter = 0;
+  if (r->graphs && !r->timing && iterations > 1) {
+    // The first iteration runs eagerly: it sizes every buffer (slab images,
+    // FFT plans) and settles volume_is_empty. One more iteration is captured
+    // on the stream and the rest replay it.
+    if ((rc = sart_iteration(r, vg, vol, voxel_type, projections, index_list, proj_count, sirt_count,
+                             volume_is_empty)))
+      return rc;
+    ++iter;
+    if (r->sart_exec) {
+      ESB_CK(cudaStreamSynchronize(r->stream), "esb_sart_run");
+      cudaGraphExecDestroy(r->sart_exec);
+      r->sart_exec = nullptr;
     }
+    // The capture records on a private stream (the caller's may be the
+    // legacy default stream, which cannot be captured); the graph is then
+    // launched on the caller's stream.
+    if (!r->capture_stream)
+      ESB_CK(cudaStreamCreateWithFlags(&r->capture_stream, cudaStreamNonBlocking), "esb_sart_run capture");
+    cudaStream_t user = r->stream;
+    if ((rc = esb_reconstructor_set_stream(r, r->capture_stream))) return rc;
+    cudaError_t e = cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      esb_reconstructor_set_stream(r, user);
+      return cuda_fail(e, "esb_sart_run capture");
+    }
+    rc = sart_iteration(r, vg, vol, voxel_type, projections, index_list, proj_count, sirt_count, volume_is_empty);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(r->stream, &graph);
+    const int rs = esb_reconstructor_set_stream(r, user);
+    if (!rc) rc = rs;
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    ESB_CK(e, "esb_sart_run capture");
+    const cudaError_t ei = cudaGraphInstantiate(&r->sart_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ESB_CK(ei, "esb_sart_run instantiate");
+    for (; iter < iterations; ++iter) ESB_CK(cudaGraphLaunch(r->sart_exec, r->stream), "esb_sart_run replay");
+    return ok();
+  }
+  for (; iter < iterations; ++iter) {
+    if ((rc = sart_iteration(r, vg, vol, voxel_type, projections, index_list, proj_count, sirt_count,
+                             volume_is_empty)))
+      return rc;
   }
   return ok();
 }

@@ -400,6 +400,11 @@ class Reconstructor:
     def enable_timing(self, on: bool = True):
         check(lib.esb_reconstructor_enable_timing(self._h, int(on)))
 
+    def enable_graphs(self, on: bool = True):
+        """Replay SART iterations 3.. of a sart() call from a CUDA graph
+        captured on iteration 2."""
+        check(lib.esb_reconstructor_enable_graphs(self._h, int(on)))
+
     def timing(self):
         """{phase: (ms, launches)} since the previous call; phases fp, bp, ctf, compare."""
         ms = np.zeros(4, np.float64)

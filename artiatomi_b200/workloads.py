@@ -29,6 +29,15 @@ CONFIGS = {
                         sirt=4, lam=0.5, iterations=2, shift=2.0, psi=0.3, snr=0.1),
     # The same geometry with a 64-voxel-thick volume (256 MiB, still larger
     # than L2): the case on which kernels are profiled with ncu.
+    # Precision at scale: 2048x2048x512, 20000 ellipsoids + 1000 beads, 61
+    # tilts of 2048^2, CTF as above, oversampling 2, 8 projections per
+    # subset, 5 iterations.
+    "c5_precision": dict(dims=(2048, 2048, 512), W=2048, H=2048, n_proj=61, n_ell=20000, n_beads=1000, ctf=True,
+                         os=2, sirt=8, lam=0.5, iterations=5, shift=2.0, psi=0.3, snr=0.1),
+    # Its 256x256x64 crop-sized counterpart for the FP64 oracle (61 tilts of
+    # 256^2, ellipsoid and bead counts scaled with the volume).
+    "c5_crop": dict(dims=(256, 256, 64), W=256, H=256, n_proj=61, n_ell=40, n_beads=2, ctf=True, os=2, sirt=8,
+                    lam=0.5, iterations=5, shift=2.0, psi=0.3, snr=0.1),
     "c2_sart_ctf_z64": dict(dims=(1024, 1024, 64), W=1024, H=1024, n_proj=61, n_ell=1250, n_beads=75, ctf=True, os=2,
                             sirt=4, lam=0.5, iterations=2, shift=2.0, psi=0.3, snr=0.1),
 }
@@ -46,6 +55,8 @@ class Workload:
     index_list: np.ndarray
     projections: object  # torch (n, H, W) float32 on the device
     phantom: object      # torch (z, y, x) float32 on the device
+    cfg_kw: dict | None = None   # ReconConfig keyword arguments
+    markers: tuple | None = None  # (tilt, x shift, y shift, psi) per projection
 
     @property
     def voxels(self) -> int:
@@ -108,4 +119,4 @@ def build(name: str, params: dict | None = None, seed: int = 0, device: str = "c
     torch.cuda.synchronize()
     rec.close()
     il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, tilt)
-    return Workload(name, p, cfg, pg, tilt, defocus, vg, il, projs, phantom)
+    return Workload(name, p, cfg, pg, tilt, defocus, vg, il, projs, phantom, cfg_kw, (tilt, xs, ys, psi))

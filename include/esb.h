@@ -325,6 +325,15 @@ int esb_reconstructor_buffers(esb_reconstructor* rec, float** proj_d, float** di
 int esb_reconstructor_enable_timing(esb_reconstructor* rec, int enable);
 int esb_reconstructor_timing(esb_reconstructor* rec, double out_ms[4], int counts[4]);
 
+/* CUDA graphs for esb_sart_run (no counterpart in the reference, which
+ * launches and synchronises every kernel from the host). When enabled and
+ * timing is off, a call with iterations > 1 runs the first iteration
+ * eagerly (sizing every buffer), captures the second on the stream and
+ * replays that graph for the remaining ones. The volume, projections, index
+ * list and subset size must stay those of the call (they are baked into the
+ * graph). */
+int esb_reconstructor_enable_graphs(esb_reconstructor* rec, int enable);
+
 /* ResetProjectionsDevice (Reconstructor.cpp:1678-1682). */
 int esb_rec_reset_projections(esb_reconstructor* rec);
 /* ForwardProjection (Reconstructor.cpp:1411-1421), CTF or not. */

@@ -304,3 +304,30 @@ def test_batched_subvolume_ragged_box_runs_per_particle():
     got = _subvolume_gpu(c, True, il)
     for b, o in zip(got, _subvolume_oracle(c, il)):
         assert rel_l2(b, o) <= 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ctf", [False, True])
+def test_sart_graph_replay_equals_eager(ctf):
+    """esb_sart_run with CUDA graphs (iteration 1 eager, 2 captured, 3.. replayed)
+    gives the eager result bit for bit: the same kernels run in the same order."""
+    import artiatomi_b200 as E
+    from tests.test_parity_recon import _ctf_cfg, _projections
+
+    case = small_case(dims=(64, 64, 24), n_proj=5, shift=0.5)
+    W, H = case["W"], case["H"]
+    n = len(case["tilt"])
+    defocus = _defocus(n, 15) if ctf else None
+    projs = cuda(_projections(case))
+    il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, case["tilt"])
+    cfgd = dict(_ctf_cfg(W), lambda_=0.5, oversampling=2) if ctf else dict(lambda_=0.5, oversampling=2)
+    vols = []
+    for graphs in (False, True):
+        rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **cfgd), case["pg"], case["tilt"], defocus)
+        rec.enable_graphs(graphs)
+        v = cuda(np.zeros(case["vol"].shape, np.float32))
+        rec.sart(case["vg"], v, projs, il, iterations=4, sirt_count=2)
+        vols.append(host(v))
+        rec.close()
+    assert np.abs(vols[0]).max() > 0
+    np.testing.assert_array_equal(vols[1], vols[0])
