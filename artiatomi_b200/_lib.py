@@ -45,6 +45,15 @@ class VolGeom(C.Structure):
                 ("z_shift", C.c_float), ("full_dim", f3), ("full_bbox_min", f3), ("full_bbox_max", f3)]
 
 
+class PrepareConfig(C.Structure):
+    _fields_ = [("input_type", C.c_int), ("wbp", C.c_int), ("normalization", C.c_int),
+                ("correct_bad_pixels", C.c_int), ("bad_pixel_value", C.c_float), ("mirror_y", C.c_int),
+                ("skip_filter", C.c_int), ("lp", C.c_float), ("hp", C.c_float), ("lps", C.c_float),
+                ("hps", C.c_float), ("dose_weighting", C.c_int), ("accumulated_dose", C.c_float),
+                ("pixel_size_nm", C.c_float), ("down_weight_tilts", C.c_int), ("tilt_deg", C.c_float),
+                ("psi_deg", C.c_float), ("wbp_filter", C.c_int)]
+
+
 class ReconConfig(C.Structure):
     _fields_ = [("proj_x", C.c_int), ("proj_y", C.c_int), ("n_proj", C.c_int), ("lambda_", C.c_float),
                 ("oversampling", C.c_int), ("ctf_mode", C.c_int), ("cut_length", C.c_float * 2),
@@ -102,6 +111,7 @@ _SIGS = {
     "esb_reconstructor_enable_timing": ([P, I], I),
     "esb_reconstructor_timing": ([P, P, P], I),
     "esb_reconstructor_enable_graphs": ([P, I], I),
+    "esb_prepare_projection": ([P, C.POINTER(PrepareConfig), P, P, C.POINTER(F), C.POINTER(F), C.POINTER(I)], I),
     "esb_rec_forward_projection": ([P, C.POINTER(VolGeom), P, I, I, I], I),
     "esb_rec_compare": ([P, C.POINTER(VolGeom), P, I], I),
     "esb_rec_back_projection": ([P, C.POINTER(VolGeom), P, I, I, F], I),

@@ -55,6 +55,13 @@ cudaError_t launch_fp_adjoint(const KConst& c, float* grad, const float* img, si
                               int h, cudaStream_t st);
 cudaError_t launch_loss_grad(const KConst& c, const void* vol, int vt, const float* meas, size_t pitchE, float sx,
                              float sy, float* grad, float* proj_out, double* out, int w, int h, cudaStream_t st);
+cudaError_t launch_convert_input(const void* in, int type, long n, float* out, cudaStream_t st);
+cudaError_t launch_window_stats(const float* img, size_t pitchE, int x0, int y0, int w, int h, double* out,
+                                cudaStream_t st);
+cudaError_t launch_bad_pixels(float* img, long n, float threshold, float value, double* out, cudaStream_t st);
+cudaError_t launch_window_div(const float* sq, size_t shift, int maxsize, int pw, int ph, float div, float* out,
+                              cudaStream_t st);
+cudaError_t launch_normalize(const float* in, float* out, long n, float mean, float std_, cudaStream_t st);
 CtfConst make_ctf_const(int n, float cs_mm, float voltage_kv, float amp_contrast, float pixel_size_nm);
 cudaError_t launch_ctf(float* spec, int n, const CtfConst& k, float d0_nm, float d1_nm, float angle_deg, int applyForFP,
                        int phaseFlip, float wiener, float4 beta, cudaStream_t st);
@@ -390,6 +397,14 @@ struct esb_reconstructor {
   bool graphs = false;                   // replay SART iterations from a captured graph
   cudaGraphExec_t sart_exec = nullptr;   // the last captured iteration
   cudaStream_t capture_stream = nullptr;  // private stream the capture records on
+  // projection preparation: square, spectrum and plans when CTF is off,
+  // the converted / windowed image and the statistics
+  float* prep_sq = nullptr;
+  float* prep_fft = nullptr;
+  float* prep_img = nullptr;
+  double* prep_stats = nullptr;
+  cufftHandle prep_r2c = 0, prep_c2r = 0;
+  bool prep_plans = false;
 };
 
 // Brackets a phase of launches with events when timing is enabled.
@@ -447,6 +462,17 @@ static void rec_free(esb_reconstructor* r) {
   if (r->capture_stream) {
     cudaStreamDestroy(r->capture_stream);
     r->capture_stream = nullptr;
+  }
+  cudaFree(r->prep_sq);
+  cudaFree(r->prep_fft);
+  cudaFree(r->prep_img);
+  cudaFree(r->prep_stats);
+  r->prep_sq = r->prep_fft = r->prep_img = nullptr;
+  r->prep_stats = nullptr;
+  if (r->prep_plans) {
+    cufftDestroy(r->prep_r2c);
+    cufftDestroy(r->prep_c2r);
+    r->prep_plans = false;
   }
   cudaFree(r->spec_batch);
   cudaFree(r->sq_batch);
@@ -916,6 +942,118 @@ static int sart_iteration(esb_reconstructor* r, const esb_vol_geom* vg, void* vo
 }
 
 extern "C" {
+
+int esb_prepare_projection(esb_reconstructor* r, const esb_prepare_config* pc, const void* in, float* out,
+                           float* mean_out, float* std_out, int* bad_out) {
+  if (!r || !pc || !in || !out) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_prepare_projection: NULL argument");
+  if (pc->input_type < ESB_PIX_F32 || pc->input_type > ESB_PIX_U32 || pc->normalization < ESB_PNM_MEAN ||
+      pc->normalization > ESB_PNM_NONE || pc->wbp_filter < 0 || pc->wbp_filter > 4)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_prepare_projection: invalid mode");
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y, N = r->N;
+  const long npx = (long)W * H, nsq = (long)N * N;
+  cudaStream_t st = r->stream;
+  // buffers (the CTF configuration already owns a square, a spectrum and plans)
+  if (!r->prep_img) ESB_CK(cudaMalloc(&r->prep_img, npx * sizeof(float)), "esb_prepare_projection");
+  if (!r->prep_stats) ESB_CK(cudaMalloc(&r->prep_stats, 4 * sizeof(double)), "esb_prepare_projection");
+  float* sq = r->square_d;
+  float* spec = r->fft_d;
+  cufftHandle r2c = r->r2c, c2r = r->c2r;
+  if (!r->plans) {
+    if (!r->prep_sq) ESB_CK(cudaMalloc(&r->prep_sq, nsq * sizeof(float)), "esb_prepare_projection");
+    if (!r->prep_fft) ESB_CK(cudaMalloc(&r->prep_fft, (size_t)(N / 2 + 1) * N * 2 * sizeof(float)), "esb_prepare_projection");
+    if (!r->prep_plans) {
+      ESB_FFT(cufftPlan2d(&r->prep_r2c, N, N, CUFFT_R2C), "esb_prepare_projection");
+      ESB_FFT(cufftPlan2d(&r->prep_c2r, N, N, CUFFT_C2R), "esb_prepare_projection");
+      r->prep_plans = true;
+    }
+    sq = r->prep_sq;
+    spec = r->prep_fft;
+    r2c = r->prep_r2c;
+    c2r = r->prep_c2r;
+  }
+  ESB_FFT(cufftSetStream(r2c, st), "esb_prepare_projection");
+  ESB_FFT(cufftSetStream(c2r, st), "esb_prepare_projection");
+  double h[4];
+  auto stats = [&](const float* img, size_t pitchE, int x0, int y0, int w, int hh) -> int {
+    ESB_CK(cudaMemsetAsync(r->prep_stats, 0, 2 * sizeof(double), st), "esb_prepare_projection");
+    ESB_CK(launch_window_stats(img, pitchE, x0, y0, w, hh, r->prep_stats, st), "esb_prepare_projection");
+    ESB_CK(cudaMemcpyAsync(h, r->prep_stats, 2 * sizeof(double), cudaMemcpyDeviceToHost, st), "esb_prepare_projection");
+    ESB_CK(cudaStreamSynchronize(st), "esb_prepare_projection");
+    return ESB_OK;
+  };
+  int rc;
+  // convert, pad (cts with fillZero = false, mirrorY for DM4: Reconstructor.cpp:1192-1204)
+  ESB_CK(launch_convert_input(in, pc->input_type, npx, out, st), "esb_prepare_projection");
+  ESB_CK(launch_make_square(W, H, W, out, N, sq, r->borderX, r->borderY, pc->mirror_y, 0, st), "esb_prepare_projection");
+  if ((rc = stats(sq, N, 0, 0, N, N))) return rc;
+  float meanValue = (float)(h[0] / (double)nsq);
+  // bad pixels (:1212-1227)
+  int bad = 0;
+  if (pc->correct_bad_pixels) {
+    ESB_CK(cudaMemsetAsync(r->prep_stats + 2, 0, sizeof(double), st), "esb_prepare_projection");
+    ESB_CK(launch_bad_pixels(sq, nsq, pc->bad_pixel_value * meanValue, meanValue, r->prep_stats + 2, st),
+           "esb_prepare_projection");
+    ESB_CK(cudaMemcpyAsync(h + 2, r->prep_stats + 2, sizeof(double), cudaMemcpyDeviceToHost, st),
+           "esb_prepare_projection");
+    ESB_CK(cudaStreamSynchronize(st), "esb_prepare_projection");
+    bad = (int)h[2];
+  }
+  float stdValue = 0.f;
+  auto mean_std = [&](double s, double q, double n, float& m, float& sd) {
+    const double mu = s / n;
+    double var = q / n - mu * mu;
+    m = (float)mu;
+    sd = (float)sqrt(var > 0.0 ? var : 0.0);
+  };
+  if (pc->wbp) {  // statistics of the raw window (:1231-1270)
+    ESB_CK(launch_window_div(sq, r->squareShift, N, W, H, 1.0f, r->prep_img, st), "esb_prepare_projection");
+    if ((rc = stats(r->prep_img, W, 0, 0, W, H))) return rc;
+    mean_std(h[0], h[1], (double)npx, meanValue, stdValue);
+    float std_hf = stdValue, mean_hf = meanValue;
+    if (pc->normalization == ESB_PNM_MEAN) std_hf = meanValue;
+    if (pc->normalization == ESB_PNM_NONE) {
+      std_hf = 1;
+      mean_hf = 0;
+    }
+    if (pc->down_weight_tilts) std_hf /= cosf(fabsf(pc->tilt_deg) / 180.0f * (float)M_PI);
+    ESB_CK(launch_normalize(r->prep_img, out, npx, mean_hf, std_hf, st), "esb_prepare_projection");
+    ESB_CK(launch_make_square(W, H, W, out, N, sq, r->borderX, r->borderY, 0, 0, st), "esb_prepare_projection");
+  }
+  float normVal = 1.0f;
+  if (!pc->skip_filter || pc->wbp) {  // (:1274-1310)
+    ESB_FFT(cufftExecR2C(r2c, (cufftReal*)sq, (cufftComplex*)spec), "esb_prepare_projection R2C");
+    if (!pc->skip_filter)
+      ESB_CK(launch_fourier_filter(spec, N, pc->lp, pc->hp, pc->lps, pc->hps, st), "esb_prepare_projection");
+    if (pc->dose_weighting)
+      ESB_CK(launch_dose_weighting(spec, N, pc->accumulated_dose, pc->pixel_size_nm * 10.0f, st),
+             "esb_prepare_projection");
+    if (pc->wbp) ESB_CK(launch_wbp_weighting(spec, N, pc->psi_deg, pc->wbp_filter, st), "esb_prepare_projection");
+    ESB_FFT(cufftExecC2R(c2r, (cufftComplex*)spec, (cufftReal*)sq), "esb_prepare_projection C2R");
+    normVal = (float)N * (float)N;
+  }
+  // normalise from the FFT (:1315-1316)
+  ESB_CK(launch_window_div(sq, r->squareShift, N, W, H, normVal, r->prep_img, st), "esb_prepare_projection");
+  if (!pc->wbp) {  // SART: statistics of the filtered window (:1320-1372)
+    if (pc->normalization == ESB_PNM_NONE) {
+      if ((rc = stats(r->prep_img, W, W / 4, H / 4, W / 2, H / 2))) return rc;
+      mean_std(h[0], h[1], (double)(W / 2) * (double)(H / 2), meanValue, stdValue);
+    } else {
+      if ((rc = stats(r->prep_img, W, 0, 0, W, H))) return rc;
+      mean_std(h[0], h[1], (double)npx, meanValue, stdValue);
+    }
+    float std_hf = stdValue, mean_hf = meanValue;
+    if (pc->normalization == ESB_PNM_MEAN) std_hf = meanValue;
+    if (pc->normalization == ESB_PNM_NONE) std_hf = 1;
+    ESB_CK(launch_normalize(r->prep_img, out, npx, mean_hf, std_hf, st), "esb_prepare_projection");
+  } else {
+    ESB_CK(cudaMemcpyAsync(out, r->prep_img, npx * sizeof(float), cudaMemcpyDeviceToDevice, st),
+           "esb_prepare_projection");
+  }
+  if (mean_out) *mean_out = meanValue;
+  if (std_out) *std_out = stdValue;
+  if (bad_out) *bad_out = bad;
+  return ok();
+}
 
 int esb_sart_run(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type, const float* projections,
                  const int* index_list, int proj_count, int iterations, int sirt_count, int* volume_is_empty) {

@@ -362,6 +362,81 @@ __global__ void k_store(const float* __restrict__ in, long n, void* __restrict__
     Voxel<VT>::store(vol, i, in[i]);
 }
 
+// ------------------------------------------------- projection preparation
+// Reconstructor::PrepareProjection (Reconstructor.cpp:1158-1383).
+
+// nppiConvert_{16s,16u,32s,32u}32f / copy: input pixels to float.
+template <typename T>
+__global__ void k_convert_input(const T* __restrict__ in, float* __restrict__ out, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  v = 0.0;
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  return v;  // valid in thread 0
+}
+
+// out[0] += sum, out[1] += sum of squares over the w x h window at (x0, y0)
+// of a pitched image, in double (nppiMean_32f_C1R / nppiMean_StdDev_32f_C1R).
+__global__ void k_window_stats(const float* __restrict__ img, size_t pitchE, int x0, int y0, int w, int h,
+                               double* __restrict__ out) {
+  const long n = (long)w * h;
+  double s = 0.0, q = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double v = img[(size_t)(y0 + i / w) * pitchE + x0 + i % w];
+    s += v;
+    q += v * v;
+  }
+  s = block_sum(s);
+  q = block_sum(q);
+  if (threadIdx.x == 0) {
+    atomicAdd(out, s);
+    atomicAdd(out + 1, q);
+  }
+}
+
+// nppiCompareC_32f_C1R(> threshold) + nppiSum_8u_C1R + nppiSet_32f_C1MR:
+// pixels above the threshold become `value`; out[0] += their count.
+__global__ void k_bad_pixels(float* __restrict__ img, long n, float threshold, float value, double* __restrict__ out) {
+  double c = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    if (img[i] > threshold) {
+      img[i] = value;
+      c += 1.0;
+    }
+  }
+  c = block_sum(c);
+  if (threadIdx.x == 0 && c > 0.0) atomicAdd(out, c);
+}
+
+// nppiDivC_32f_C1R on the centred W x H window of the square:
+// out = sq[window] / div.
+__global__ void k_window_div(const float* __restrict__ sq, size_t shift, int maxsize, int pw, int ph, float div,
+                             float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= pw || y >= ph) return;
+  out[(size_t)y * pw + x] = sq[shift + (size_t)y * maxsize + x] / div;
+}
+
+// nppiSubC_32f_C1R then nppiDivC_32f_C1IR(-std): out = (in - mean) / (-std).
+__global__ void k_normalize(const float* __restrict__ in, float* __restrict__ out, long n, float mean, float std_) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = (in[i] - mean) / (-std_);
+}
+
 // ----------------------------------------------------------------- launchers
 static inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
 
@@ -426,6 +501,50 @@ cudaError_t launch_square_to_image_batch(const float* sq, int count, int maxsize
 cudaError_t launch_transpose(const float* in, int w, int h, size_t pitchE, float* out, cudaStream_t st) {
   dim3 b(32, 8), g((w + 31) / 32, (h + 31) / 32);
   k_transpose<<<g, b, 0, st>>>(in, w, h, pitchE, out); ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+static inline int grid1(long n) {
+  long b = (n + 255) / 256;
+  return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+cudaError_t launch_convert_input(const void* in, int type, long n, float* out, cudaStream_t st) {
+  switch (type) {
+    case ESB_PIX_S16: k_convert_input<int16_t><<<grid1(n), 256, 0, st>>>((const int16_t*)in, out, n); break;
+    case ESB_PIX_U16: k_convert_input<uint16_t><<<grid1(n), 256, 0, st>>>((const uint16_t*)in, out, n); break;
+    case ESB_PIX_S32: k_convert_input<int32_t><<<grid1(n), 256, 0, st>>>((const int32_t*)in, out, n); break;
+    case ESB_PIX_U32: k_convert_input<uint32_t><<<grid1(n), 256, 0, st>>>((const uint32_t*)in, out, n); break;
+    default: k_convert_input<float><<<grid1(n), 256, 0, st>>>((const float*)in, out, n); break;
+  }
+  ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_window_stats(const float* img, size_t pitchE, int x0, int y0, int w, int h, double* out,
+                                cudaStream_t st) {
+  k_window_stats<<<grid1((long)w * h), 256, 0, st>>>(img, pitchE, x0, y0, w, h, out);
+  ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bad_pixels(float* img, long n, float threshold, float value, double* out, cudaStream_t st) {
+  k_bad_pixels<<<grid1(n), 256, 0, st>>>(img, n, threshold, value, out);
+  ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_window_div(const float* sq, size_t shift, int maxsize, int pw, int ph, float div, float* out,
+                              cudaStream_t st) {
+  dim3 b(32, 8);
+  k_window_div<<<grid2(pw, ph, b), b, 0, st>>>(sq, shift, maxsize, pw, ph, div, out);
+  ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_normalize(const float* in, float* out, long n, float mean, float std_, cudaStream_t st) {
+  k_normalize<<<grid1(n), 256, 0, st>>>(in, out, n, mean, std_);
+  ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 

@@ -412,6 +412,32 @@ class Reconstructor:
         check(lib.esb_reconstructor_timing(self._h, fptr(ms), fptr(cnt)))
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("fp", "bp", "ctf", "compare"))}
 
+    def prepare_projection(self, raw, out, **pc):
+        """PrepareProjection (Reconstructor.cpp:1158-1383): raw projection
+        (device tensor: float32, int16, uint16, int32 or uint32) -> normalised
+        float image `out`. Keyword arguments are the fields of
+        esb_prepare_config (input_type is taken from raw's dtype). Returns
+        (mean, std, bad_pixels)."""
+        import torch
+
+        kinds = {torch.float32: 0, torch.int16: 1, torch.int32: 3}
+        try:
+            kinds[torch.uint16] = 2
+            kinds[torch.uint32] = 4
+        except AttributeError:
+            pass
+        c = L.PrepareConfig()
+        c.input_type = kinds[raw.dtype]
+        c.normalization = 1
+        c.correct_bad_pixels = 1
+        c.bad_pixel_value = 10.0
+        for k, v in pc.items():
+            setattr(c, k, v)
+        m, s, b = C.c_float(), C.c_float(), C.c_int()
+        check(lib.esb_prepare_projection(self._h, C.byref(c), fptr(raw), fptr(out), C.byref(m), C.byref(s),
+                                         C.byref(b)))
+        return m.value, s.value, b.value
+
     def forward_projection(self, vg, vol, index: int, volume_is_empty: bool = False):
         check(lib.esb_rec_forward_projection(self._h, C.byref(vg), fptr(vol), _voxel_type_of(vol), index,
                                              int(volume_is_empty)))

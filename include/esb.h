@@ -345,6 +345,51 @@ int esb_rec_compare(esb_reconstructor* rec, const esb_vol_geom* vg, const float*
 int esb_rec_back_projection(esb_reconstructor* rec, const esb_vol_geom* vg, void* vol, int voxel_type, int index,
                             float sirt_count);
 
+/* Reconstructor::PrepareProjection (Reconstructor.cpp:1158-1383): the raw
+ * projection `in` (device, W x H, input_type) becomes the normalised float
+ * image `out` (device, W x H) that the reconstruction reads:
+ *   convert to float; pad to the N x N square (mirror padding, flipped in y
+ *   for DM4 stacks); mean of the square; bad pixels (> bad_pixel_value *
+ *   mean) set to the mean; WBP: normalise the raw window (mean / std /
+ *   none, std divided by cos(tilt) with down_weight_tilts) and pad again;
+ *   unless skip_filter (or WBP): R2C, band-pass (lp, hp, lps, hps), dose
+ *   weighting, WBP weighting (psi, wbp_filter), C2R, / N^2; SART: normalise
+ *   the filtered window (mean / std over the whole image, or the centre half
+ *   for ESB_PNM_NONE, which keeps the mean and divides by 1):
+ *   out = (x - mean) / (-std).
+ * mean, std (host, may be NULL) receive the statistics the reference
+ * returns, bad_pixels (host, may be NULL) the count. Synchronises the
+ * reconstructor's stream (the statistics are read back, as the reference
+ * does). Statistics are FP64 sums; the reference's NPP reductions are not
+ * pinned. */
+#define ESB_PIX_F32 0
+#define ESB_PIX_S16 1
+#define ESB_PIX_U16 2
+#define ESB_PIX_S32 3
+#define ESB_PIX_U32 4
+#define ESB_PNM_MEAN 0
+#define ESB_PNM_STANDARD_DEV 1
+#define ESB_PNM_NONE 2
+typedef struct {
+  int input_type;          /* ESB_PIX_* (ProjectionSource data type) */
+  int wbp;                 /* WBP_NoSART */
+  int normalization;       /* ProjectionNormalization: ESB_PNM_* */
+  int correct_bad_pixels;  /* CorrectBadPixels */
+  float bad_pixel_value;   /* BadPixelValue */
+  int mirror_y;            /* FileReadMode == FRM_DM4 */
+  int skip_filter;         /* SkipFilter */
+  float lp, hp, lps, hps;  /* fourFilterLP, fourFilterHP, fourFilterLPS, fourFilterHPS */
+  int dose_weighting;      /* DoseWeighting */
+  float accumulated_dose;  /* AccumulatedDose[index] */
+  float pixel_size_nm;     /* Projection::GetPixelSize() */
+  int down_weight_tilts;   /* DownWeightTiltsForWBP */
+  float tilt_deg;          /* marker tilt angle of the projection */
+  float psi_deg;           /* marker psi of the projection */
+  int wbp_filter;          /* WBPFilter: FM_RAMP 0 .. FM_CONTRAST30 4 */
+} esb_prepare_config;
+int esb_prepare_projection(esb_reconstructor* rec, const esb_prepare_config* pc, const void* in, float* out,
+                           float* mean, float* std_dev, int* bad_pixels);
+
 /* The SART driver loop of EmSart.cpp:579-675 for one GPU: iterations x
  * ordered subsets of sirt_count projections x {FP, compare} then {BP}.
  * projections: device, n_proj images of W x H (already prepared);

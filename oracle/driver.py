@@ -221,3 +221,70 @@ class OracleReconstructor:
                         continue
                     g = G.orc_geom(pair_geoms[p][index], sub_geoms[p], self.aniso, self.aniso_inv, for_bp=True)
                     bp(g, box, 0, filt, 1.0, c["oversampling"], ray, ray1, 1, self.precision, self.q9)
+
+
+def _mean_std(a):
+    a = np.asarray(a, np.float64)
+    mu = a.sum() / a.size
+    var = (a * a).sum() / a.size - mu * mu
+    return np.float32(mu), np.float32(np.sqrt(max(var, 0.0)))
+
+
+def prepare_projection(raw, N, pc: dict):
+    """Reconstructor::PrepareProjection (Reconstructor.cpp:1158-1383) on one
+    raw W x H projection; pc has the fields of esb_prepare_config. Returns
+    (normalised float image, mean, std, bad pixel count). Mean and standard
+    deviation are FP64 sums (population variance), where the reference calls
+    NPP."""
+    H, W = raw.shape
+    bx, by = (N - W) // 2, (N - H) // 2
+    img = np.ascontiguousarray(raw.astype(np.float32))
+    sq = make_square(img, N, bx, by, int(pc.get("mirror_y", 0)), 0)
+    meanValue = np.float32(sq.astype(np.float64).sum() / sq.size)
+    bad = 0
+    if pc.get("correct_bad_pixels", 0):
+        mask = sq > np.float32(np.float32(pc["bad_pixel_value"]) * meanValue)
+        bad = int(mask.sum())
+        sq[mask] = meanValue
+    stdValue = np.float32(0)
+    norm = pc.get("normalization", 1)
+    if pc.get("wbp", 0):
+        win = np.ascontiguousarray(sq[by:by + H, bx:bx + W] / np.float32(1.0))
+        meanValue, stdValue = _mean_std(win)
+        std_hf, mean_hf = stdValue, meanValue
+        if norm == 0:
+            std_hf = meanValue
+        if norm == 2:
+            std_hf, mean_hf = np.float32(1), np.float32(0)
+        if pc.get("down_weight_tilts", 0):
+            std_hf = np.float32(std_hf / np.float32(np.cos(np.float32(abs(pc["tilt_deg"])) / np.float32(180.0) *
+                                                            np.float32(np.pi))))
+        out = ((win - mean_hf) / (-std_hf)).astype(np.float32)
+        sq = make_square(np.ascontiguousarray(out), N, bx, by, 0, 0)
+    normVal = np.float32(1.0)
+    if not pc.get("skip_filter", 0) or pc.get("wbp", 0):
+        spec = r2c(sq)
+        if not pc.get("skip_filter", 0):
+            olib.orc_fourier_filter(addr(spec), N, pc.get("lp", 0.0), pc.get("hp", 0.0), pc.get("lps", 0.0),
+                                    pc.get("hps", 0.0))
+        if pc.get("dose_weighting", 0):
+            olib.orc_dose_weighting(addr(spec), N, pc["accumulated_dose"], np.float32(pc["pixel_size_nm"]) *
+                                    np.float32(10.0))
+        if pc.get("wbp", 0):
+            olib.orc_wbp_weighting(addr(spec), N, pc.get("psi_deg", 0.0), pc.get("wbp_filter", 0))
+        sq = c2r(spec)
+        normVal = np.float32(N) * np.float32(N)
+    win = (sq[by:by + H, bx:bx + W] / normVal).astype(np.float32)
+    if pc.get("wbp", 0):
+        return np.ascontiguousarray(win), meanValue, stdValue, bad
+    if norm == 2:
+        meanValue, stdValue = _mean_std(win[H // 4:H // 4 + H // 2, W // 4:W // 4 + W // 2])
+    else:
+        meanValue, stdValue = _mean_std(win)
+    std_hf, mean_hf = stdValue, meanValue
+    if norm == 0:
+        std_hf = meanValue
+    if norm == 2:
+        std_hf = np.float32(1)
+    out = ((win - mean_hf) / (-std_hf)).astype(np.float32)
+    return np.ascontiguousarray(out), meanValue, stdValue, bad
