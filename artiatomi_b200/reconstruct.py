@@ -1,0 +1,101 @@
+"""EmSART's reconstruction run (EmSart.cpp main, SART and WBP) on libesb.
+
+`reconstruct(cfg)` reads the tilt series, marker file and CTF file named by
+an `EmSartConfig` (emsart.cfg), prepares every usable projection on the GPU
+(Reconstructor::PrepareProjection), runs SART (or WBP: one back-projection
+per projection of the filtered images, EmSart.cpp:575-583, 624-629) and
+writes the volume as EmSart.cpp:694-813 does (negated FP32, or FP16 when
+FP16Volume and WriteVolumeAsFP16 are set). Every computation runs in the
+library's CUDA kernels; this module only moves files and buffers.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import emsart as E
+from . import fileio as F
+from .config import EmSartConfig
+
+_PIX = {np.dtype(np.float32): "float32", np.dtype(np.int16): "int16", np.dtype(np.uint16): "uint16",
+        np.dtype(np.int32): "int32", np.dtype(np.uint32): "uint32"}
+
+
+def reconstruct(cfg: EmSartConfig, write: bool = True, variant: int = E.VARIANT_FAST, graphs: bool = True):
+    """Runs the configured reconstruction; returns the volume as written
+    ([z][y][x], numpy) and the Reconstructor statistics per projection."""
+    import torch
+
+    dev = torch.device("cuda", cfg.CudaDeviceID[0] if cfg.CudaDeviceID else 0)
+    torch.cuda.set_device(dev)
+    stack, pixel_nm = F.read_stack(cfg.ProjectionFile)
+    if stack.dtype not in _PIX:
+        raise TypeError("Projections have wrong data type: supported types are: short, ushort, int, uint and float.")
+    n, H, W = stack.shape
+    md = F.read_markers(cfg.MarkerFile, cfg.ReferenceMarker)
+    if md.projection_count != n:
+        raise ValueError(f"marker file has {md.projection_count} projections, the stack {n}")
+    markers = md.markers()
+    tc = E.TiltConfig(cfg.AddTiltAngle, cfg.AddTiltXAngle, cfg.UseFixPsiAngle, cfg.PsiAngle, cfg.PhiAngle)
+    pg = E.projection_geometry(markers, W, H, tc)
+    vg = E.volume_geometry(cfg.RecDimensions, cfg.VoxelSize, cfg.VolumeShift)
+    amount, angle = cfg.MagAnisotropy
+    mag = E.mag_aniso_matrix(amount, angle, W, H)
+    mag_inv = E.mag_aniso_matrix(1.0 / amount, angle, W, H)
+    defocus = F.read_ctf(cfg.CtfFile).ravel() if cfg.CtfMode else None
+    rc = E.ReconConfig(W, H, n, lambda_=cfg.Lambda, oversampling=cfg.OverSampling, ctf_mode=cfg.CtfMode,
+                       cut_length=cfg.CutLength, dim_length=cfg.DimLength, crop=cfg.Crop, crop_dim=cfg.CropDim,
+                       projection_scale_factor=cfg.ProjectionScaleFactor, pixel_size_nm=pixel_nm, cs_mm=cfg.Cs,
+                       voltage_kv=cfg.Voltage, amp_contrast=0.0, ctf_slice_thickness_nm=cfg.CTFSliceThickness,
+                       ctf_beta_fac=cfg.CTFBetaFac, wiener_noise_level=cfg.WienerFilterNoiseLevel,
+                       phase_flip_only=cfg.PhaseFlipOnly, ignore_z_shift_for_ctf=cfg.IgnoreZShiftForCTF,
+                       switch_ctf_direction=cfg.SwitchCTFDirectionForIMOD, volume_shift=cfg.VolumeShift,
+                       add_tilt_angle=cfg.AddTiltAngle, variant=variant)
+    tilt = markers.tilt_angle
+    rec = E.Reconstructor(rc, pg, tilt, defocus, mag, mag_inv)
+    good = md.good()
+    # PrepareProjection for every usable projection (EmSart.cpp:534-572)
+    prepared = torch.zeros((n, H, W), dtype=torch.float32, device=dev)
+    stats = []
+    psi = markers.rotation_psi
+    for i in range(n):
+        if not good[i]:
+            stats.append(None)
+            continue
+        raw = torch.from_numpy(np.ascontiguousarray(stack[i])).to(dev)
+        pc = dict(wbp=int(cfg.WBP), normalization=cfg.ProjectionNormalization,
+                  correct_bad_pixels=int(cfg.CorrectBadPixels), bad_pixel_value=cfg.BadPixelValue,
+                  mirror_y=int(cfg.ProjectionFile.rfind(".dm4") >= 0), skip_filter=int(cfg.SkipFilter),
+                  lp=float(cfg.fourFilterLP), hp=float(cfg.fourFilterHP), lps=float(cfg.fourFilterLPS),
+                  hps=float(cfg.fourFilterHPS), dose_weighting=int(cfg.DoseWeighting),
+                  accumulated_dose=float(cfg.AccumulatedDose[i]) if cfg.DoseWeighting else 0.0,
+                  pixel_size_nm=pixel_nm, down_weight_tilts=int(cfg.DownWeightTiltsForWBP),
+                  tilt_deg=float(tilt[i]), psi_deg=float(psi[i] if psi is not None else 0.0),
+                  wbp_filter=cfg.WBPFilter)
+        stats.append(rec.prepare_projection(raw, prepared[i], **pc))
+    index_list = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, tilt, good.astype(np.int32))
+    vol = torch.zeros(tuple(int(d) for d in cfg.RecDimensions[::-1]), device=dev,
+                      dtype=torch.float16 if cfg.FP16Volume else torch.float32)
+    if cfg.WBP:  # one back-projection of every filtered projection (EmSart.cpp:575-583, 624-651)
+        proj_v, _, _ = rec.views()
+        for index in index_list:
+            proj_v.copy_(prepared[int(index)])
+            rec.back_projection(vg, vol, int(index), 1.0)
+    else:
+        rec.enable_graphs(graphs)
+        rec.sart(vg, vol, prepared, index_list, iterations=cfg.Iterations, sirt_count=cfg.SIRTCount,
+                 volume_is_empty=True)
+    torch.cuda.synchronize()
+    # output (EmSart.cpp:694-813): FP32 volumes are negated (Volume::Invert),
+    # FP16 volumes too when converted to float (convertVolumeFP16ToFP32,
+    # BackProjectionSquareOS.cu:1296-1323), FP16 output is written as stored
+    if cfg.FP16Volume and cfg.WriteVolumeAsFP16:
+        out = vol.cpu().numpy()
+    else:
+        neg = torch.empty(vol.shape, dtype=torch.float32, device=dev)
+        E.convert_volume(vol, neg, negate=True)
+        torch.cuda.synchronize()
+        out = neg.cpu().numpy()
+    rec.close()
+    if write:
+        F.write_volume(cfg.OutVolumeFile, out, pixel_nm, cfg.VoxelSize[0])
+    return out, stats
