@@ -97,9 +97,20 @@ class EmSartConfig:
     MagAnisotropy: tuple = (1.0, 0.0)
     IgnoreZShiftForCTF: bool = False
     CTFSliceThickness: float = 50.0
+    # EmSARTSubVolumes (SUBVOLREC_MODE keys of utils/Config.cpp:479-494)
+    SizeSubVol: int = 0
+    VoxelSizeSubVol: float = 0.0
+    MotiveList: str = ""
+    SubVolPath: str = ""
+    ShiftInputFile: str = ""
+    BatchSize: int = 0
+    MaxShift: int = 0
+    NamingConvention: int = 0  # NC_ParticleOnly, 1 NC_TomogramParticle
+    ScaleMotivelistShift: float = 1.0
+    ScaleMotivelistPosition: float = 1.0
 
     @classmethod
-    def from_text(cls, text: str) -> "EmSartConfig":
+    def from_text(cls, text: str, subvolumes: bool = False) -> "EmSartConfig":
         s = parse_config(text)
         c = cls()
 
@@ -175,11 +186,22 @@ class EmSartConfig:
             c.MagAnisotropy = (m[0], m[1])
         c.IgnoreZShiftForCTF = _bool(opt("IgnoreZShiftForCTF", "false"))
         c.CTFSliceThickness = float(opt("CTFSliceThickness", "50"))
+        if subvolumes:
+            c.SizeSubVol = int(float(req("SizeSubVol")))
+            c.VoxelSizeSubVol = float(req("VoxelSizeSubVol"))
+            c.MotiveList = req("MotiveList")
+            c.SubVolPath = req("SubVolPath")
+            c.ShiftInputFile = req("ShiftInputFile")
+            c.BatchSize = int(float(req("BatchSize")))
+            c.MaxShift = int(float(req("MaxShift")))
+            c.NamingConvention = 1 if opt("NamingConvention", "") in ("TomoParticle", "Tomo_Particle") else 0
+            c.ScaleMotivelistShift = float(req("ScaleMotivelistShift"))
+            c.ScaleMotivelistPosition = float(req("ScaleMotivelistPosition"))
         return c
 
     @classmethod
-    def from_file(cls, path: str) -> "EmSartConfig":
+    def from_file(cls, path: str, subvolumes: bool = False) -> "EmSartConfig":
         with open(path) as f:
-            return cls.from_text(f.read())
+            return cls.from_text(f.read(), subvolumes)
 
 

@@ -25,6 +25,14 @@ The layouts are the reference's (they define the files users already have):
 * CTF file (src/EmTools/FileIO/CtfFile.cpp): an EM float file of
   projections columns; row 1 holds the minimum defocus, row 2 the maximum
   (nm), row 4 the astigmatism angle (rad).
+* Motive list (src/EmTools/FileIO/MotiveListe.h, MotiveList.cpp): an EM
+  float file of 20 x particles (cc, x/y click, particle nr, tomogram nr,
+  particle nr in tomogram, wedge, x/y/z coordinate, x/y/z shift, shifts
+  before, phi, psi, theta, class); coordinates and shifts are scaled by the
+  binning factors at read.
+* Shift file (src/EmTools/FileIO/ShiftFile.cpp): an EM float file of
+  motives x projections x 2; the extra shift of (projection, motive) is the
+  negated stored pair.
 """
 from __future__ import annotations
 
@@ -264,6 +272,50 @@ def write_ctf(path: str, defocus_min, defocus_max, astig_rad) -> None:
     d = np.zeros((5, n), np.float32)
     d[1], d[2], d[4] = defocus_min, defocus_max, astig_rad
     write_em(path, d[None])
+
+
+# ------------------------------------------------------------ motive list
+MOTL_FIELDS = ["ccCoeff", "xCoord", "yCoord", "partNr", "tomoNr", "partNrInTomo", "wedgeIdx", "x_Coord", "y_Coord",
+               "z_Coord", "x_Shift", "y_Shift", "z_Shift", "x_ShiftBefore", "y_ShiftBefore", "z_ShiftBefore", "phi",
+               "psi", "theta", "classNo"]
+
+
+def read_motive_list(path: str, scale_position: float = 1.0, scale_shift: float = 1.0) -> np.ndarray:
+    """Particles [n][20] (MotiveList::GetAt: click coordinates and x/y/z
+    coordinates times scale_position, x/y/z shifts times scale_shift)."""
+    data, _ = read_em(path)
+    if data.shape[2] != 20:
+        raise ValueError(f"{path}: not a motive list (DimX = {data.shape[2]}, expected 20)")
+    m = data.reshape(-1, 20).astype(np.float32).copy()
+    for k in (1, 2, 7, 8, 9):
+        m[:, k] *= np.float32(scale_position)
+    for k in (10, 11, 12):
+        m[:, k] *= np.float32(scale_shift)
+    return m
+
+
+def write_motive_list(path: str, particles: np.ndarray) -> None:
+    write_em(path, np.ascontiguousarray(particles, np.float32).reshape(1, -1, 20))
+
+
+def index_coding(particle: np.ndarray, tomo_particle: bool = False) -> str:
+    """motive::GetIndexCoding: the particle number (or tomogram_particle),
+    formatted as a C++ stream formats a float."""
+    def g(v):
+        return "%g" % float(np.float32(v))
+
+    return f"{g(particle[4])}_{g(particle[5])}" if tomo_particle else g(particle[3])
+
+
+def read_shift_file(path: str) -> np.ndarray:
+    """Extra shifts [projection][motive][2] (ShiftFile::operator(): negated)."""
+    data, _ = read_em(path)  # [2][projections][motives]
+    return np.ascontiguousarray(-np.moveaxis(data.astype(np.float32), 0, -1))
+
+
+def write_shift_file(path: str, stored: np.ndarray) -> None:
+    """stored [2][projections][motives] as the file holds it."""
+    write_em(path, np.ascontiguousarray(stored, np.float32))
 
 
 def exists(path: str) -> bool:

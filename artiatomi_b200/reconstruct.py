@@ -5,13 +5,18 @@ an `EmSartConfig` (emsart.cfg), prepares every usable projection on the GPU
 (Reconstructor::PrepareProjection), runs SART (or WBP: one back-projection
 per projection of the filtered images, EmSart.cpp:575-583, 624-629) and
 writes the volume as EmSart.cpp:694-813 does (negated FP32, or FP16 when
-FP16Volume and WriteVolumeAsFP16 are set). Every computation runs in the
-library's CUDA kernels; this module only moves files and buffers.
+FP16Volume and WriteVolumeAsFP16 are set). `reconstruct_subvolumes(cfg)`
+is EmSartSubVolumes' run: the particle boxes of a motive list with their
+per-tilt extra shifts. Every computation runs in the library's CUDA
+kernels; this module only moves files and buffers.
 """
 from __future__ import annotations
 
+from dataclasses import dataclass
+
 import numpy as np
 
+from . import _lib as L
 from . import emsart as E
 from . import fileio as F
 from .config import EmSartConfig
@@ -20,9 +25,26 @@ _PIX = {np.dtype(np.float32): "float32", np.dtype(np.int16): "int16", np.dtype(n
         np.dtype(np.int32): "int32", np.dtype(np.uint32): "uint32"}
 
 
-def reconstruct(cfg: EmSartConfig, write: bool = True, variant: int = E.VARIANT_FAST, graphs: bool = True):
-    """Runs the configured reconstruction; returns the volume as written
-    ([z][y][x], numpy) and the Reconstructor statistics per projection."""
+@dataclass
+class _Run:
+    rec: object
+    pg: object
+    vg: object
+    markers: object
+    tilt: np.ndarray
+    good: np.ndarray
+    prepared: object
+    stats: list
+    pixel_nm: float
+    tc: object
+    dev: object
+    W: int
+    H: int
+
+
+def _setup(cfg: EmSartConfig, variant: int) -> _Run:
+    """Files in, geometry, reconstructor and the prepared projections
+    (EmSart.cpp / EmSartSubVolumes.cpp up to the reconstruction loop)."""
     import torch
 
     dev = torch.device("cuda", cfg.CudaDeviceID[0] if cfg.CudaDeviceID else 0)
@@ -72,17 +94,27 @@ def reconstruct(cfg: EmSartConfig, write: bool = True, variant: int = E.VARIANT_
                   tilt_deg=float(tilt[i]), psi_deg=float(psi[i] if psi is not None else 0.0),
                   wbp_filter=cfg.WBPFilter)
         stats.append(rec.prepare_projection(raw, prepared[i], **pc))
-    index_list = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, tilt, good.astype(np.int32))
+    return _Run(rec, pg, vg, markers, tilt, good, prepared, stats, pixel_nm, tc, dev, W, H)
+
+
+def reconstruct(cfg: EmSartConfig, write: bool = True, variant: int = E.VARIANT_FAST, graphs: bool = True):
+    """Runs the configured reconstruction; returns the volume as written
+    ([z][y][x], numpy) and the Reconstructor statistics per projection."""
+    import torch
+
+    R = _setup(cfg, variant)
+    rec, vg, dev = R.rec, R.vg, R.dev
+    index_list = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, R.tilt, R.good.astype(np.int32))
     vol = torch.zeros(tuple(int(d) for d in cfg.RecDimensions[::-1]), device=dev,
                       dtype=torch.float16 if cfg.FP16Volume else torch.float32)
     if cfg.WBP:  # one back-projection of every filtered projection (EmSart.cpp:575-583, 624-651)
         proj_v, _, _ = rec.views()
         for index in index_list:
-            proj_v.copy_(prepared[int(index)])
+            proj_v.copy_(R.prepared[int(index)])
             rec.back_projection(vg, vol, int(index), 1.0)
     else:
         rec.enable_graphs(graphs)
-        rec.sart(vg, vol, prepared, index_list, iterations=cfg.Iterations, sirt_count=cfg.SIRTCount,
+        rec.sart(vg, vol, R.prepared, index_list, iterations=cfg.Iterations, sirt_count=cfg.SIRTCount,
                  volume_is_empty=True)
     torch.cuda.synchronize()
     # output (EmSart.cpp:694-813): FP32 volumes are negated (Volume::Invert),
@@ -91,11 +123,63 @@ def reconstruct(cfg: EmSartConfig, write: bool = True, variant: int = E.VARIANT_
     if cfg.FP16Volume and cfg.WriteVolumeAsFP16:
         out = vol.cpu().numpy()
     else:
-        neg = torch.empty(vol.shape, dtype=torch.float32, device=dev)
-        E.convert_volume(vol, neg, negate=True)
-        torch.cuda.synchronize()
-        out = neg.cpu().numpy()
+        out = _negated(vol, dev)
     rec.close()
     if write:
-        F.write_volume(cfg.OutVolumeFile, out, pixel_nm, cfg.VoxelSize[0])
-    return out, stats
+        F.write_volume(cfg.OutVolumeFile, out, R.pixel_nm, cfg.VoxelSize[0])
+    return out, R.stats
+
+
+def _negated(vol, dev):
+    import torch
+
+    neg = torch.empty(vol.shape, dtype=torch.float32, device=dev)
+    E.convert_volume(vol, neg, negate=True)
+    torch.cuda.synchronize()
+    return neg.cpu().numpy()
+
+
+def reconstruct_subvolumes(cfg: EmSartConfig, write: bool = True, batched: bool = True,
+                           variant: int = E.VARIANT_FAST):
+    """EmSartSubVolumes' run (EmSartSubVolumes.cpp:611-705): weighted
+    back-projection of a SizeSubVol^3 box around every particle of the motive
+    list, each projection shifted by the particle's extra shift from the
+    shift file (tilts with |shift| >= MaxShift - 0.5 are left out), BatchSize
+    particles per pass, every box written negated to
+    SubVolPath + <particle index coding> + ".em". Returns {file name: box}."""
+    import torch
+
+    R = _setup(cfg, variant)
+    rec, vg, dev = R.rec, R.vg, R.dev
+    motl = F.read_motive_list(cfg.MotiveList, cfg.ScaleMotivelistPosition, cfg.ScaleMotivelistShift)
+    shifts = F.read_shift_file(cfg.ShiftInputFile)  # [projection][motive][2]
+    n_part = motl.shape[0]
+    n_proj = len(R.tilt)
+    index_list = E.projection_index_list(E.PLT_NORMAL, R.tilt, R.good.astype(np.int32))
+    batch = max(1, cfg.BatchSize)
+    S = cfg.SizeSubVol
+    out = {}
+    for b0 in range(0, n_part, batch):
+        parts = list(range(b0, min(b0 + batch, n_part)))
+        sub, boxes = [], []
+        pair = (L.ProjGeom * (len(parts) * n_proj))()
+        active = np.zeros((len(parts), n_proj), np.uint8)
+        for k, p in enumerate(parts):
+            m = motl[p]
+            sub.append(E.subvolume_geometry(S, cfg.VoxelSizeSubVol, vg, m[7:10], m[10:13]))
+            es = shifts[:, p, :]  # [projection][2]
+            g = E.projection_geometry(R.markers, R.W, R.H, R.tc, extra_shift=es)
+            for i in range(n_proj):
+                pair[k * n_proj + i] = g[i]
+            active[k] = np.sqrt((es.astype(np.float32) ** 2).sum(1)) < np.float32(cfg.MaxShift - 0.5)
+            boxes.append(torch.zeros((S, S, S), dtype=torch.float32, device=dev))
+        rec.subvolume_wbp(vg, sub, pair, boxes, R.prepared, index_list, active=active, batched=batched)
+        torch.cuda.synchronize()
+        for k, p in enumerate(parts):
+            name = cfg.SubVolPath + F.index_coding(motl[p], cfg.NamingConvention == 1) + ".em"
+            box = _negated(boxes[k], dev)
+            out[name] = box
+            if write:
+                F.write_em(name, box)
+    rec.close()
+    return out

@@ -21,7 +21,7 @@ REF_ROOT = Path(os.environ.get("REF_ROOT", "/root/reference"))
 TOOLS = REF_ROOT / "src" / "EmTools"
 SOURCES = ["FileIO/EmFile.cpp", "FileIO/MRCFile.cpp", "FileIO/File.cpp", "FileIO/FileReader.cpp",
            "FileIO/FileWriter.cpp", "FileIO/FileIOException.cpp", "FileIO/ImageBase.cpp", "FileIO/MarkerFile.cpp",
-           "FileIO/CtfFile.cpp", "FileIO/ImodFiducialFile.cpp", "FilterGraph/Matrix.cpp", "FilterGraph/PointF.cpp",
+           "FileIO/CtfFile.cpp", "FileIO/ImodFiducialFile.cpp", "FileIO/MotiveList.cpp", "FileIO/ShiftFile.cpp", "FilterGraph/Matrix.cpp", "FilterGraph/PointF.cpp",
            "Minimization/levmar.cpp"]
 
 

@@ -12,6 +12,8 @@
 //   ref_fileio write_mrc FILE nx ny nz ps    float ramp data, MRCFile writer
 //   ref_fileio markers FILE ref              per projection: tilt xshift yshift mag psi good
 //   ref_fileio ctf FILE n                    per projection: min max angle
+//   ref_fileio motl FILE scale_pos scale_shift  per particle: coords, shifts, index coding
+//   ref_fileio shifts FILE                   per projection and motive: extra shift x y
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -21,6 +23,8 @@
 #include "EmFile.h"
 #include "MRCFile.h"
 #include "MarkerFile.h"
+#include "MotiveListe.h"
+#include "ShiftFile.h"
 
 static double sum_of(void* data, DataType_enum t, size_t n) {
   double s = 0;
@@ -81,6 +85,25 @@ int main(int argc, char** argv) {
     CtfFile c(path);
     for (int i = 0; i < atoi(argv[3]); ++i)
       printf("%.9g %.9g %.9g\n", c.GetMinDefocus(i), c.GetMaxDefocus(i), c.GetAstigmatismAngle(i));
+    return 0;
+  }
+  if (op == "motl" && argc >= 5) {
+    MotiveList ml(path, (float)atof(argv[3]), (float)atof(argv[4]));
+    for (int i = 0; i < ml.GetParticleCount(); ++i) {
+      motive m = ml.GetAt(i);
+      printf("%.9g %.9g %.9g %.9g %.9g %.9g %s %s\n", m.x_Coord, m.y_Coord, m.z_Coord, m.x_Shift, m.y_Shift,
+             m.z_Shift, m.GetIndexCoding(MotiveList::NC_ParticleOnly).c_str(),
+             m.GetIndexCoding(MotiveList::NC_TomogramParticle).c_str());
+    }
+    return 0;
+  }
+  if (op == "shifts") {
+    ShiftFile sf(path);
+    for (int p = 0; p < sf.GetProjectionCount(); ++p)
+      for (int m = 0; m < sf.GetMotiveCount(); ++m) {
+        my_float2 v = sf(p, m);
+        printf("%.9g %.9g\n", v.x, v.y);
+      }
     return 0;
   }
   return 2;

@@ -56,6 +56,18 @@ def make_files(d: Path) -> dict:
     p = d / "ours_ctf.em"
     F.write_ctf(str(p), [3000.0, 3100.0, 3200.0], [3050.0, 3150.0, 3250.0], [0.1, 1.2, -0.4])
     out[p.name] = p
+    motl = np.zeros((3, 20), np.float32)
+    motl[:, 3] = [1, 2, 1234567]
+    motl[:, 4], motl[:, 5] = [7, 7, 8], [3, 4, 12.5]
+    motl[:, 7:10] = [[10.5, 20, 30], [40, 50.25, 60], [70, 80, 90.75]]
+    motl[:, 10:13] = [[0.5, -0.25, 1], [0, 0, 0], [-2, 1.5, 0.125]]
+    p = d / "ours_motl.em"
+    F.write_motive_list(str(p), motl)
+    out[p.name] = p
+    stored = (np.arange(2 * 4 * 3, dtype=np.float32).reshape(2, 4, 3) - 10.0) * 0.25
+    p = d / "ours_shifts.em"
+    F.write_shift_file(str(p), stored)
+    out[p.name] = p
     return out
 
 
@@ -66,6 +78,10 @@ def reference_report(exe: Path, files: dict) -> dict:
             args = ["markers", str(p), "1"]
         elif name == "ours_ctf.em":
             args = ["ctf", str(p), "3"]
+        elif name == "ours_motl.em":
+            args = ["motl", str(p), "2", "0.5"]
+        elif name == "ours_shifts.em":
+            args = ["shifts", str(p)]
         else:
             args = ["read", str(p)]
         rep[name] = subprocess.run([str(exe), *args], check=True, capture_output=True, text=True).stdout

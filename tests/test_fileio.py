@@ -56,6 +56,17 @@ def _check_reports(reports, files):
             d = F.read_ctf(str(p))
             rows = np.array([list(map(float, ln.split())) for ln in text.strip().splitlines()])
             np.testing.assert_allclose(d, rows, rtol=1e-6, atol=1e-5)
+        elif name == "ours_motl.em":
+            m = F.read_motive_list(str(p), 2.0, 0.5)
+            for i, ln in enumerate(text.strip().splitlines()):
+                v = ln.split()
+                np.testing.assert_allclose(m[i, 7:13], list(map(float, v[:6])), rtol=1e-7)
+                assert F.index_coding(m[i]) == v[6]
+                assert F.index_coding(m[i], tomo_particle=True) == v[7]
+        elif name == "ours_shifts.em":
+            sh = F.read_shift_file(str(p))  # [projection][motive][2]
+            rows = np.array([list(map(float, ln.split())) for ln in text.strip().splitlines()])
+            np.testing.assert_array_equal(sh.reshape(-1, 2), rows.astype(np.float32))
         else:
             vals = text.split()
             a = F.read_em(str(p))[0] if name.endswith(".em") else F.read_mrc(str(p))[0]

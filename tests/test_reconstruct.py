@@ -103,3 +103,67 @@ def test_reconstruct_matches_oracle(tmp_path, wbp):
     ref = _oracle_run(cfg, raw, tilt, psi, og, vo)
     assert np.abs(ref).max() > 0
     assert rel_l2(out, ref) <= 1e-3, rel_l2(out, ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("batched", [False, True])
+def test_reconstruct_subvolumes_matches_oracle(tmp_path, batched):
+    """EmSartSubVolumes' run from config, motive list and shift file against
+    the oracle's sub-volume WBP on the oracle-prepared projections."""
+    import artiatomi_b200 as E
+    from artiatomi_b200 import fileio as F
+    from artiatomi_b200.config import EmSartConfig
+    from artiatomi_b200.reconstruct import reconstruct_subvolumes
+    from oracle import geometry as G
+    from oracle.driver import OracleReconstructor, prepare_projection
+
+    raw, tilt, psi, og, vo = _dataset(tmp_path, wbp=True)
+    rng = np.random.default_rng(12)
+    n_part, S = 5, 16
+    motl = np.zeros((n_part, 20), np.float32)
+    motl[:, 3] = np.arange(1, n_part + 1)
+    motl[:, 7:10] = np.stack([rng.uniform(20, 44, n_part), rng.uniform(20, 44, n_part), rng.uniform(8, 16, n_part)], 1)
+    motl[:, 10:13] = rng.uniform(-1, 1, (n_part, 3))
+    F.write_motive_list(str(tmp_path / "motl.em"), motl)
+    stored = rng.uniform(-1.8, 1.8, (2, N, n_part)).astype(np.float32)
+    F.write_shift_file(str(tmp_path / "shifts.em"), stored)
+    (tmp_path / "sub").mkdir()
+    text = (tmp_path / "emsart.cfg").read_text() + f"""SizeSubVol = {S}
+VoxelSizeSubVol = 1
+MotiveList = {tmp_path / 'motl.em'}
+SubVolPath = {tmp_path / 'sub'}/
+ShiftInputFile = {tmp_path / 'shifts.em'}
+BatchSize = 3
+MaxShift = 2
+ScaleMotivelistShift = 1
+ScaleMotivelistPosition = 1
+"""
+    cfg = EmSartConfig.from_text(text, subvolumes=True)
+    got = reconstruct_subvolumes(cfg, batched=batched)
+    assert sorted(got) == sorted(str(tmp_path / "sub" / f"{i}.em") for i in range(1, n_part + 1))
+    # oracle
+    pc = dict(wbp=1, normalization=cfg.ProjectionNormalization, correct_bad_pixels=1,
+              bad_pixel_value=cfg.BadPixelValue, skip_filter=int(cfg.SkipFilter), lp=float(cfg.fourFilterLP),
+              hp=float(cfg.fourFilterHP), lps=float(cfg.fourFilterLPS), hps=float(cfg.fourFilterHPS),
+              wbp_filter=cfg.WBPFilter)
+    prepared = np.stack([prepare_projection(raw[i], max(W, H), dict(pc, tilt_deg=float(tilt[i]),
+                                                                    psi_deg=float(psi[i])))[0]
+                         for i in range(N)])
+    xs = F.read_markers(cfg.MarkerFile).item("X_Shift")
+    ys = F.read_markers(cfg.MarkerFile).item("Y_Shift")
+    es = -np.moveaxis(stored, 0, -1)  # [projection][motive][2]
+    subo = [G.subvolume_geometry(S, 1.0, vo, motl[p, 7:10], motl[p, 10:13]) for p in range(n_part)]
+    pair_o = [G.projection_geometry(tilt, xs, ys, None, psi, W, H, extra_shift=es[:, p, :]) for p in range(n_part)]
+    active = (np.sqrt((es ** 2).sum(2)).T < 1.5).astype(np.uint8)
+    cfgd = dict(lambda_=cfg.Lambda, oversampling=cfg.OverSampling, cut_length=cfg.CutLength,
+                dim_length=cfg.DimLength)
+    orc = OracleReconstructor(cfgd, W, H, og, tilt, precision=1)
+    bo = [np.zeros((S, S, S), np.float32) for _ in range(n_part)]
+    il = E.projection_index_list(E.PLT_NORMAL, tilt)
+    orc.subvolume_wbp(vo, subo, pair_o, bo, prepared, il, active=active)
+    for p in range(n_part):
+        name = str(tmp_path / "sub" / f"{p + 1}.em")
+        box = F.read_em(name)[0]
+        np.testing.assert_array_equal(box, got[name])
+        assert np.abs(bo[p]).max() > 0
+        assert rel_l2(box, -bo[p]) <= 1e-3, (p, rel_l2(box, -bo[p]))
