@@ -148,15 +148,20 @@ __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float
   float nzs = dqz > 0.f ? (fz + 1.f - pz) * isz : (dqz < 0.f ? (pz - fz) * isz : inf);
   const int stx = dqx > 0.f ? 1 : -1, stz = dqz > 0.f ? 1 : -1;
   const float ib = 1.0f - b;
-  const long y0 = (long)(iy < 0 ? 0 : (iy > C.ny - 1 ? C.ny - 1 : iy)) * C.sy;
-  const long y1 = (long)(iy + 1 < 0 ? 0 : (iy + 1 > C.ny - 1 ? C.ny - 1 : iy + 1)) * C.sy;
-  auto ey = [&](int x, int z) {
-    x = x < 0 ? 0 : (x > C.nx - 1 ? C.nx - 1 : x);
-    z = z < 0 ? 0 : (z > C.nz - 1 ? C.nz - 1 : z);
-    const long o = (long)z * C.sz + x;
-    return ib * Voxel<VT>::load(C.vol, o + y0) + b * Voxel<VT>::load(C.vol, o + y1);
+  // Corner reads without per-load clamping or 64-bit index arithmetic: the
+  // clamped x columns and z rows of the current cell are kept (each step
+  // clamps only the one new index), and element offsets are 32-bit (volumes
+  // of up to 2^32 voxels; launch_project_fast checks).
+  const unsigned sz = (unsigned)C.sz;
+  const unsigned y0 = (unsigned)(iy < 0 ? 0 : (iy > C.ny - 1 ? C.ny - 1 : iy)) * (unsigned)C.sy;
+  const unsigned y1 = (unsigned)(iy + 1 < 0 ? 0 : (iy + 1 > C.ny - 1 ? C.ny - 1 : iy + 1)) * (unsigned)C.sy;
+  auto clampx = [&](int x) { return (unsigned)(x < 0 ? 0 : (x > C.nx - 1 ? C.nx - 1 : x)); };
+  auto clampz = [&](int z) { return (unsigned)(z < 0 ? 0 : (z > C.nz - 1 ? C.nz - 1 : z)) * sz; };
+  auto ey = [&](unsigned xo, unsigned zo) {
+    return ib * Voxel<VT>::load(C.vol, (long)(zo + y0 + xo)) + b * Voxel<VT>::load(C.vol, (long)(zo + y1 + xo));
   };
-  float e00 = ey(ix, iz), e10 = ey(ix + 1, iz), e01 = ey(ix, iz + 1), e11 = ey(ix + 1, iz + 1);
+  unsigned x0 = clampx(ix), x1 = clampx(ix + 1), z0 = clampz(iz), z1 = clampz(iz + 1);
+  float e00 = ey(x0, z0), e10 = ey(x1, z0), e01 = ey(x0, z1), e11 = ey(x1, z1);
   const int M_total = J - j0;
   int m0 = 0;
   float acc = 0.0f;
@@ -182,21 +187,29 @@ __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float
       ix += stx;
       nxs = stx > 0 ? ((float)(ix + 1) - px) * isx : (px - (float)ix) * isx;
       if (stx > 0) {
+        x0 = x1;
+        x1 = clampx(ix + 1);
         e00 = e10; e01 = e11;
-        e10 = ey(ix + 1, iz); e11 = ey(ix + 1, iz + 1);
+        e10 = ey(x1, z0); e11 = ey(x1, z1);
       } else {
+        x1 = x0;
+        x0 = clampx(ix);
         e10 = e00; e11 = e01;
-        e00 = ey(ix, iz); e01 = ey(ix, iz + 1);
+        e00 = ey(x0, z0); e01 = ey(x0, z1);
       }
     } else {
       iz += stz;
       nzs = stz > 0 ? ((float)(iz + 1) - pz) * isz : (pz - (float)iz) * isz;
       if (stz > 0) {
+        z0 = z1;
+        z1 = clampz(iz + 1);
         e00 = e01; e10 = e11;
-        e01 = ey(ix, iz + 1); e11 = ey(ix + 1, iz + 1);
+        e01 = ey(x0, z1); e11 = ey(x1, z1);
       } else {
+        z1 = z0;
+        z0 = clampz(iz);
         e01 = e00; e11 = e10;
-        e00 = ey(ix, iz); e10 = ey(ix + 1, iz);
+        e00 = ey(x0, z0); e10 = ey(x1, z0);
       }
     }
   }
@@ -352,6 +365,7 @@ cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float*
                                 size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1,
                                 cudaStream_t st) {
   if (x1 <= x0 || y1 <= y0 || slabs.count <= 0) return cudaSuccess;
+  if ((double)c.dim.x * c.dim.y * c.dim.z > 4294967295.0) return cudaErrorInvalidValue;  // 32-bit voxel offsets
   dim3 blk(256), grd((x1 - x0 + 7) / 8, (y1 - y0 + 7) / 8);
   if (vt == ESB_VOXEL_F32)
     k_slicer_fused<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
@@ -367,6 +381,7 @@ cudaError_t launch_project_fast(const KConst& c, const void* vol, int vt, int mo
                                 size_t pitchE, float tmin, float tmax, int x0, int y0, int x1, int y1,
                                 cudaStream_t st) {
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
+  if ((double)c.dim.x * c.dim.y * c.dim.z > 4294967295.0) return cudaErrorInvalidValue;  // 32-bit voxel offsets
   dim3 blk(256), grd((x1 - x0 + 7) / 8, (y1 - y0 + 7) / 8);
 #define ESB_LAUNCH(VT, M)                                                                            \
   do {                                                                                               \
