@@ -162,30 +162,35 @@ __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float
   };
   unsigned x0 = clampx(ix), x1 = clampx(ix + 1), z0 = clampz(iz), z1 = clampz(iz + 1);
   float e00 = ey(x0, z0), e10 = ey(x1, z0), e01 = ey(x0, z1), e11 = ey(x1, z1);
-  const int M_total = J - j0;
-  int m0 = 0;
+  // Integer counters that feed float arithmetic are kept as floats as well
+  // (exact: all values are below 2^24), so the loop converts nothing.
+  const float Mt = (float)(J - j0);
+  const float fj0 = (float)j0;
+  float fm0 = 0.0f;
+  float fix = (float)ix, fiz = (float)iz;
+  const float fstx = (float)stx, fstz = (float)stz;
   float acc = 0.0f;
 #pragma unroll 1
   for (int guard = 0; guard < 1 << 20; ++guard) {
     const float sexit = fminf(nxs, nzs);
-    int m1 = (sexit >= (float)M_total) ? M_total : (int)ceilf(sexit);
-    if (m1 > M_total) m1 = M_total;
-    if (m1 > m0) {
-      const float a0 = __fsub_rn(qpos(qx, j0 + m0, dqx), (float)ix);
-      const float c0 = __fsub_rn(qpos(qz, j0 + m0, dqz), (float)iz);
-      const float M = (float)(m1 - m0);
+    const float fm1 = (sexit >= Mt) ? Mt : ceilf(sexit);
+    if (fm1 > fm0) {
+      const float a0 = __fsub_rn(__fmaf_rn(fj0 + fm0, dqx, qx), fix);
+      const float c0 = __fsub_rn(__fmaf_rn(fj0 + fm0, dqz, qz), fiz);
+      const float M = fm1 - fm0;
       const float S1 = 0.5f * M * (M - 1.f);
       const float S2 = S1 * (2.f * M - 1.f) * (1.f / 3.f);
       const float k1 = e10 - e00, k3 = e01 - e00, k5 = e11 - e10 - e01 + e00;
       const float sa = M * a0 + S1 * dqx, sc = M * c0 + S1 * dqz;
       const float sac = M * a0 * c0 + S1 * (a0 * dqz + c0 * dqx) + S2 * dqx * dqz;
       acc += e00 * M + k1 * sa + k3 * sc + k5 * sac;
-      m0 = m1;
+      fm0 = fm1;
     }
-    if (m0 >= M_total) break;
+    if (fm0 >= Mt) break;
     if (nxs <= nzs) {
       ix += stx;
-      nxs = stx > 0 ? ((float)(ix + 1) - px) * isx : (px - (float)ix) * isx;
+      fix += fstx;
+      nxs = stx > 0 ? ((fix + 1.0f) - px) * isx : (px - fix) * isx;
       if (stx > 0) {
         x0 = x1;
         x1 = clampx(ix + 1);
@@ -199,7 +204,8 @@ __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float
       }
     } else {
       iz += stz;
-      nzs = stz > 0 ? ((float)(iz + 1) - pz) * isz : (pz - (float)iz) * isz;
+      fiz += fstz;
+      nzs = stz > 0 ? ((fiz + 1.0f) - pz) * isz : (pz - fiz) * isz;
       if (stz > 0) {
         z0 = z1;
         z1 = clampz(iz + 1);
