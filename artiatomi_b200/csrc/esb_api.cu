@@ -30,7 +30,11 @@ cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img,
                            float lambda, int os, float distMin, float distMax, int linear, cudaStream_t st);
 cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
                                  const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
-                                 float distMin, float distMax, int linear, cudaStream_t st, int transposed);
+                                 float distMin, float distMax, int linear, cudaStream_t st, int transposed,
+                                 const float* ups = nullptr, size_t up_stride = 0);
+cudaError_t launch_upsample(const float* imgs, size_t img_stride, int count, int pw, int ph, int os, int linear,
+                            float* up, size_t up_stride, cudaStream_t st);
+bool bp_can_upsample(const KConst& k, int os);
 cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float* imgs, size_t img_stride,
                                 size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1, cudaStream_t st);
 cudaError_t launch_compare(int pw, int ph, size_t pitchE, const float* real, float* virt, const float* dist,
@@ -386,6 +390,8 @@ struct esb_reconstructor {
   PhaseTimer timers[4];
   float* slab_imgs = nullptr;  // per-slab images of the fused CTF paths
   size_t slab_cap = 0;         // capacity in images
+  float* up_imgs = nullptr;    // the slab images pre-sampled on the sub-pixel grid
+  size_t up_cap = 0;           // capacity in floats
   SubvolBatch batch;           // tables of the batched sub-volume launch
   // filtered spectra and squares of a chunk of CTF slabs, with a batched
   // C2R plan per chunk size
@@ -453,6 +459,9 @@ static void rec_free(esb_reconstructor* r) {
   cudaFree(r->slab_imgs);
   r->slab_imgs = nullptr;
   r->slab_cap = 0;
+  cudaFree(r->up_imgs);
+  r->up_imgs = nullptr;
+  r->up_cap = 0;
   subvol_batch_free(r->batch);
   if (r->sart_exec) {
     cudaStreamSynchronize(r->stream);
@@ -736,6 +745,35 @@ static int rec_subvol_slab_images(esb_reconstructor* r, const esb_vol_geom* full
   return ESB_OK;
 }
 
+// Pre-samples `count` transposed slab images for the back-projection
+// (launch_upsample); returns NULL when the geometry does not allow it
+// (oversampling not a power of two, magnification anisotropy) or the
+// images would exceed 4 GiB, and the back-projection then filters the slab
+// images itself. `up_stride` receives the floats per pre-sampled image.
+static const float* rec_upsample(esb_reconstructor* r, const KConst& c, int count, int linear, size_t& up_stride) {
+  const esb_recon_config& cf = r->cfg;
+  const int os = cf.oversampling;
+  up_stride = (size_t)cf.proj_x * os * (size_t)cf.proj_y * os;
+  const size_t need = up_stride * (size_t)count;
+  if (!bp_can_upsample(c, os) || need * sizeof(float) > ((size_t)4 << 30)) return nullptr;
+  if (need > r->up_cap) {
+    if (cudaStreamSynchronize(r->stream) != cudaSuccess) return nullptr;
+    cudaFree(r->up_imgs);
+    r->up_imgs = nullptr;
+    r->up_cap = 0;
+    if (cudaMalloc(&r->up_imgs, need * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    r->up_cap = need;
+  }
+  const size_t img = (size_t)cf.proj_x * cf.proj_y;
+  if (launch_upsample(r->slab_imgs, img, count, cf.proj_x, cf.proj_y, os, linear, r->up_imgs, up_stride, r->stream) !=
+      cudaSuccess)
+    return nullptr;
+  return r->up_imgs;
+}
+
 extern "C" {
 
 int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, const void* vol, int voxel_type, int index,
@@ -855,8 +893,11 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
       SlabTable none;
       none.count = 0;
       PhaseScope ps(r, 1);
+      size_t up_stride = 0;
+      const float* up = rec_upsample(r, c, 1, 0, up_stride);
+      ESB_CK(cudaGetLastError(), "back projection");
       ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, 0, none, W, H, W, lambda, cf.oversampling, 0.0f,
-                                  9999999999999.0f, 0, r->stream, 1), "back projection");
+                                  9999999999999.0f, 0, r->stream, 1, up, up_stride), "back projection");
       return ESB_OK;
     }
     PhaseScope ps(r, 1);
@@ -883,8 +924,11 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
       if ((rc = rec_ctf_chain(r, img, 1, p, index, dmin, dmax, 0, r->slab_imgs + k * npx, nullptr, 1, p, 1))) return rc;
     }
     PhaseScope ps(r, 1);
+    size_t up_stride = 0;
+    const float* up = rec_upsample(r, c, T.count, 1, up_stride);
+    ESB_CK(cudaGetLastError(), "back projection");
     ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, npx, T, W, H, W, lambda, cf.oversampling, 0.f, 0.f,
-                                1, r->stream, 1), "back projection");
+                                1, r->stream, 1, up, up_stride), "back projection");
     return ESB_OK;
   }
   for (float ray = t_in; ray < t_out; ray += step) {

@@ -35,7 +35,8 @@ template <int VT>
 __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __restrict__ vol,
                                                  const float* __restrict__ imgs, size_t img_stride, SlabTable slabs,
                                                  int pw, int ph, size_t pitchE, float lambda, int os, float inv,
-                                                 float distMin, float distMax, int linear, int transposed) {
+                                                 float distMin, float distMax, int linear, int transposed,
+                                                 const float* __restrict__ ups, size_t up_stride) {
   const int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int z = (int)blockIdx.z;
@@ -46,11 +47,13 @@ __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __res
   int pbx, pby, pbz, pbw;
   macro_footprint(k, x, y, z, pw, ph, depth, pbx, pby, pbz, pbw);
   const float* img = imgs;
+  const float* up = ups;
   if (slabs.count > 0) {  // fused CTF slabs
     if (!(depth >= slabs.bound[0] && depth < slabs.bound[slabs.count])) return;
     int s = 0;
     while (s + 1 < slabs.count && depth >= slabs.bound[s + 1]) ++s;
     img = imgs + (size_t)s * img_stride;
+    if (up) up += (size_t)s * up_stride;
   } else if (!(depth >= distMin && depth < distMax)) {
     return;
   }
@@ -59,7 +62,7 @@ __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __res
 #pragma unroll
   for (int i = 0; i < 4; ++i)
     voxel_sums(k, g, img, pw, ph, pitchE, os, inv, linear != 0, transposed != 0, x + i, y, z, pbx, pby, pbz, pbw,
-               acc[i], dacc[i]);
+               acc[i], dacc[i], up, ph * os);
   if (VT == ESB_VOXEL_F32 && (((uintptr_t)((float*)vol + base)) & 15) == 0) {
     float4 v = *((float4*)((float*)vol + base));
     if (dacc[0] > 0.f) v.x += lambda * acc[0] / dacc[0];
@@ -75,20 +78,38 @@ __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __res
   }
 }
 
+// The slab images (transposed, [x][y], stride img_stride) sampled at every
+// sub-pixel grid point: up[s][mu][mv] = image s at ((mu + 0.5) / os,
+// (mv + 0.5) / os), clamp addressing, nearest or bilinear as the
+// back-projection reads it.
+__global__ void __launch_bounds__(256) k_upsample(const float* __restrict__ imgs, size_t img_stride, int pw, int ph,
+                                                  int os, float inv, int linear, float* __restrict__ up,
+                                                  size_t up_stride) {
+  const int mv = blockIdx.x * blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  const int s = blockIdx.z;
+  const int upH = ph * os;
+  if (mv >= upH) return;
+  const float px = ((float)mu + 0.5f) * inv, py = ((float)mv + 0.5f) * inv;
+  up[(size_t)s * up_stride + (size_t)mu * upH + mv] =
+      sample_image(imgs + (size_t)s * img_stride, pw, ph, (size_t)pw, px, py, linear != 0, true);
+}
+
 }  // namespace
 
 cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
                                  const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
-                                 float distMin, float distMax, int linear, cudaStream_t st, int transposed) {
+                                 float distMin, float distMax, int linear, cudaStream_t st, int transposed,
+                                 const float* ups, size_t up_stride) {
   const int nq = k.dimXQuarter, ny = (int)k.dim.y, nz = (int)k.dim.z;
   if (nq <= 0 || ny <= 0 || nz <= 0) return cudaSuccess;
   const BpGeom g = make_geom(k, os);
   const float inv = 1.0f / (float)os;
   dim3 blk(32, 4, 1), grd((nq + 31) / 32, (ny + 3) / 4, nz);
   switch (vt) {
-    case ESB_VOXEL_F32: k_bp_fast<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); ESB_COUNT_LAUNCH(); break;
-    case ESB_VOXEL_F16: k_bp_fast<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); ESB_COUNT_LAUNCH(); break;
-    default: k_bp_fast<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed); ESB_COUNT_LAUNCH(); break;
+    case ESB_VOXEL_F32: k_bp_fast<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed, ups, up_stride); ESB_COUNT_LAUNCH(); break;
+    case ESB_VOXEL_F16: k_bp_fast<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed, ups, up_stride); ESB_COUNT_LAUNCH(); break;
+    default: k_bp_fast<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed, ups, up_stride); ESB_COUNT_LAUNCH(); break;
   }
   return cudaGetLastError();
 }
@@ -97,7 +118,27 @@ cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img,
                            float lambda, int os, float distMin, float distMax, int linear, cudaStream_t st) {
   SlabTable none;
   none.count = 0;
-  return launch_bp_fast_slabs(k, vol, vt, img, 0, none, pw, ph, pitchE, lambda, os, distMin, distMax, linear, st, 0);
+  return launch_bp_fast_slabs(k, vol, vt, img, 0, none, pw, ph, pitchE, lambda, os, distMin, distMax, linear, st, 0,
+                              nullptr, 0);
+}
+
+// Pre-sampled slab images for k_bp_fast (transposed input images, up_stride
+// floats per output image of (pw * os) x (ph * os)).
+cudaError_t launch_upsample(const float* imgs, size_t img_stride, int count, int pw, int ph, int os, int linear,
+                            float* up, size_t up_stride, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  dim3 blk(256), grd((ph * os + 255) / 256, pw * os, count);
+  k_upsample<<<grd, blk, 0, st>>>(imgs, img_stride, pw, ph, os, 1.0f / (float)os, linear, up, up_stride);
+  ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+// Whether k_bp_fast may read pre-sampled images: the sub-pixel recurrence is
+// exact (power-of-two oversampling) and samples are read at (px, py) (no
+// magnification anisotropy).
+bool bp_can_upsample(const KConst& k, int os) {
+  const BpGeom g = make_geom(k, os);
+  return g.exact_grid && g.aniso_identity;
 }
 
 }  // namespace esb

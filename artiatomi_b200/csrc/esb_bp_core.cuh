@@ -147,10 +147,16 @@ __device__ __forceinline__ float sample_interior(const float* __restrict__ img, 
 // pbw <= ph - 1, so a nearest-texel read never leaves the image and a
 // bilinear read only does so below a lower edge: with no anisotropy the
 // clamps are skipped unless pbx or pbz is 0 under bilinear interpolation.
+//
+// up (may be NULL): the image pre-sampled at every point of the sub-pixel
+// grid, up[mu][mv] = image at ((mu + 0.5) / os, (mv + 0.5) / os) with row
+// length upH = ph * os (k_upsample). With a power-of-two oversampling and no
+// anisotropy the recurrence visits exactly those points, so each sample is
+// one load instead of a filtered read.
 __device__ __forceinline__ void voxel_sums(const KConst& k, const BpGeom& g, const float* __restrict__ img, int pw,
                                            int ph, size_t pitchE, int os, float inv, bool linear, bool transposed,
                                            int x, int y, int z, int pbx, int pby, int pbz, int pbw, float& acc,
-                                           float& dacc) {
+                                           float& dacc, const float* __restrict__ up = nullptr, int upH = 0) {
   const float cx = k.bbMin.x + ((float)x + 0.5f) * k.vs.x, cy = k.bbMin.y + ((float)y + 0.5f) * k.vs.y,
               cz = k.bbMin.z + ((float)z + 0.5f) * k.vs.z;
   const float uc = g.U.x * cx + g.U.y * cy + g.U.z * cz + g.U0;
@@ -164,6 +170,31 @@ __device__ __forceinline__ void voxel_sums(const KConst& k, const BpGeom& g, con
   const float du0 = px0 - uc;
   // in-plane offset d = du * u + dv * v, advanced by inv * u per sample
   const float ix = inv * g.u.x, iy = inv * g.u.y, iz = inv * g.u.z;
+  if (up) {
+    const float fos = (float)os;
+    const size_t mu0 = (size_t)(int)(px0 * fos - 0.5f);  // exact: px0 = (mu0 + 0.5) / os
+#pragma unroll 1
+    for (float py = py0; py < (float)pbw && py <= vb; py = fadd(py, inv)) {
+      const float dv = py - vc;
+      float dx = du0 * g.u.x + dv * g.v.x, dy = du0 * g.u.y + dv * g.v.y, dz = du0 * g.u.z + dv * g.v.z;
+      const float* p = up + mu0 * (size_t)upH + (size_t)(int)(py * fos - 0.5f);
+#pragma unroll 1
+      for (float px = px0; px < (float)pby && px <= ub; px = fadd(px, inv)) {
+        const float L = chord(dx, dy, dz, g);
+        if (L > 0.0f) {
+          a += __ldg(p) * L;
+          da += L;
+        }
+        dx += ix;
+        dy += iy;
+        dz += iz;
+        p += upH;
+      }
+    }
+    acc = a;
+    dacc = da;
+    return;
+  }
 #pragma unroll 1
   for (float py = py0; py < (float)pbw && py <= vb; py = fadd(py, inv)) {
     const float dv = py - vc;
