@@ -66,6 +66,16 @@ cudaError_t launch_bad_pixels(float* img, long n, float threshold, float value, 
 cudaError_t launch_window_div(const float* sq, size_t shift, int maxsize, int pw, int ph, float div, float* out,
                               cudaStream_t st);
 cudaError_t launch_normalize(const float* in, float* out, long n, float mean, float std_, cudaStream_t st);
+cudaError_t launch_crop_to_square_batch(int pw, int ph, float* images, size_t img_stride, int count, int apply_crop,
+                                        int seq_crop, float2 cut, float2 dim, const int* p, int maxsize, float* sq,
+                                        size_t sq_stride, int bx, int by, cudaStream_t st);
+cudaError_t launch_ctf_batch(float* spec, size_t spec_stride, int n, const CtfConst& k, const CtfSlabs& slabs_nm,
+                             float angle_deg, int applyForFP, int phaseFlip, float wiener, float4 beta,
+                             cudaStream_t st);
+cudaError_t launch_square_to_image_many(const float* sq, size_t sq_stride, int count, int maxsize, size_t shift,
+                                        float inv_norm, int pw, int ph, float* out, size_t out_stride, float* accum,
+                                        int apply_crop, float2 cut, float2 dim, const int* p, int transpose_out,
+                                        cudaStream_t st);
 CtfConst make_ctf_const(int n, float cs_mm, float voltage_kv, float amp_contrast, float pixel_size_nm);
 cudaError_t launch_ctf(float* spec, int n, const CtfConst& k, float d0_nm, float d1_nm, float angle_deg, int applyForFP,
                        int phaseFlip, float wiener, float4 beta, cudaStream_t st);
@@ -400,6 +410,8 @@ struct esb_reconstructor {
   int batch_slabs = 0;
   cufftHandle c2r_many[ESB_CTF_SLAB_BATCH + 1] = {};
   bool c2r_many_ok[ESB_CTF_SLAB_BATCH + 1] = {};
+  cufftHandle r2c_many[ESB_CTF_SLAB_BATCH + 1] = {};
+  bool r2c_many_ok[ESB_CTF_SLAB_BATCH + 1] = {};
   bool graphs = false;                   // replay SART iterations from a captured graph
   cudaGraphExec_t sart_exec = nullptr;   // the last captured iteration
   cudaStream_t capture_stream = nullptr;  // private stream the capture records on
@@ -487,11 +499,16 @@ static void rec_free(esb_reconstructor* r) {
   cudaFree(r->sq_batch);
   r->spec_batch = r->sq_batch = nullptr;
   r->batch_slabs = 0;
-  for (int i = 0; i <= ESB_CTF_SLAB_BATCH; ++i)
+  for (int i = 0; i <= ESB_CTF_SLAB_BATCH; ++i) {
     if (r->c2r_many_ok[i]) {
       cufftDestroy(r->c2r_many[i]);
       r->c2r_many_ok[i] = false;
     }
+    if (r->r2c_many_ok[i]) {
+      cufftDestroy(r->r2c_many[i]);
+      r->r2c_many_ok[i] = false;
+    }
+  }
 }
 
 extern "C" {
@@ -545,8 +562,10 @@ int esb_reconstructor_set_stream(esb_reconstructor* rec, void* stream) {
   if (rec->plans) {
     ESB_FFT(cufftSetStream(rec->r2c, rec->stream), "esb_reconstructor_set_stream");
     ESB_FFT(cufftSetStream(rec->c2r, rec->stream), "esb_reconstructor_set_stream");
-    for (int i = 0; i <= ESB_CTF_SLAB_BATCH; ++i)
+    for (int i = 0; i <= ESB_CTF_SLAB_BATCH; ++i) {
       if (rec->c2r_many_ok[i]) ESB_FFT(cufftSetStream(rec->c2r_many[i], rec->stream), "esb_reconstructor_set_stream");
+      if (rec->r2c_many_ok[i]) ESB_FFT(cufftSetStream(rec->r2c_many[i], rec->stream), "esb_reconstructor_set_stream");
+    }
   }
   return ok();
 }
@@ -687,6 +706,81 @@ static int rec_slab_capacity(esb_reconstructor* r, int count) {
   return ESB_OK;
 }
 
+// Chunk buffers of the batched CTF chains: `want` spectra and squares.
+static int rec_batch_buffers(esb_reconstructor* r, int want) {
+  const int N = r->N;
+  if (want <= r->batch_slabs) return ESB_OK;
+  const size_t spec = (size_t)(N / 2 + 1) * N * 2, sq = (size_t)N * N;
+  ESB_CK(cudaStreamSynchronize(r->stream), "CTF slab buffers");
+  cudaFree(r->spec_batch);
+  cudaFree(r->sq_batch);
+  r->spec_batch = r->sq_batch = nullptr;
+  r->batch_slabs = 0;
+  ESB_CK(cudaMalloc(&r->spec_batch, (size_t)want * spec * sizeof(float)), "CTF slab buffers");
+  ESB_CK(cudaMalloc(&r->sq_batch, (size_t)want * sq * sizeof(float)), "CTF slab buffers");
+  r->batch_slabs = want;
+  return ESB_OK;
+}
+
+// Batched N x N transforms of `cnt` squares / spectra (one plan per count).
+static int rec_fft_many(esb_reconstructor* r, int cnt, bool forward) {
+  const int N = r->N;
+  cufftHandle* plans = forward ? r->r2c_many : r->c2r_many;
+  bool* ok = forward ? r->r2c_many_ok : r->c2r_many_ok;
+  if (!ok[cnt]) {
+    int dims[2] = {N, N};
+    ESB_FFT(cufftPlanMany(&plans[cnt], 2, dims, nullptr, 1, 0, nullptr, 1, 0, forward ? CUFFT_R2C : CUFFT_C2R, cnt),
+            "CTF slab plan");
+    ok[cnt] = true;
+    ESB_FFT(cufftSetStream(plans[cnt], r->stream), "CTF slab plan");
+  }
+  if (forward)
+    ESB_FFT(cufftExecR2C(plans[cnt], (cufftReal*)r->sq_batch, (cufftComplex*)r->spec_batch), "CTF slab R2C");
+  else
+    ESB_FFT(cufftExecC2R(plans[cnt], (cufftComplex*)r->spec_batch, (cufftReal*)r->sq_batch), "CTF slab C2R");
+  return ESB_OK;
+}
+
+// The CTF chain of rec_ctf_chain for every slab of table T, ESB_CTF_SLAB_BATCH
+// slabs per batched transform. Inputs: the slab images (seq_crop = 0,
+// images + k * img, cropped in place when crop_in) or one image cropped again
+// before every slab (seq_crop = 1, the back-projection's residual). Outputs:
+// image k written to out + k * img (transposed when transpose_out) and/or
+// all slabs added to accum in slab order.
+static int rec_ctf_chain_slabs(esb_reconstructor* r, const SlabTable& T, int index, float* images, int seq_crop,
+                               int crop_in, const int* p_in, int for_fp, float* out, float* accum, int crop_out,
+                               const int* p_out, int transpose_out) {
+  const esb_recon_config& cf = r->cfg;
+  const int W = cf.proj_x, H = cf.proj_y, N = r->N;
+  const size_t img = (size_t)W * H, spec = (size_t)(N / 2 + 1) * N * 2, sq = (size_t)N * N;
+  int rc;
+  if ((rc = rec_batch_buffers(r, std::min(T.count, ESB_CTF_SLAB_BATCH)))) return rc;
+  const float2 cut = make_float2(cf.cut_length[0], cf.cut_length[1]);
+  const float2 dim = make_float2(cf.dim_length[0], cf.dim_length[1]);
+  const float4 beta = make_float4(cf.ctf_beta_fac[0], cf.ctf_beta_fac[1], cf.ctf_beta_fac[2], cf.ctf_beta_fac[3]);
+  PhaseScope ps(r, 2);
+  for (int c0 = 0; c0 < T.count; c0 += ESB_CTF_SLAB_BATCH) {
+    const int cnt = std::min(ESB_CTF_SLAB_BATCH, T.count - c0);
+    CtfSlabs S;
+    S.count = cnt;
+    for (int j = 0; j < cnt; ++j)
+      esb_defocus_min_max(T.bound[c0 + j], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
+                          cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
+                          cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &S.d0[j], &S.d1[j]);
+    ESB_CK(launch_crop_to_square_batch(W, H, seq_crop ? images : images + (size_t)c0 * img, img, cnt, crop_in, seq_crop,
+                                       cut, dim, p_in, N, r->sq_batch, sq, r->borderX, r->borderY, r->stream),
+           "CTF slab chain");
+    if ((rc = rec_fft_many(r, cnt, true))) return rc;
+    ESB_CK(launch_ctf_batch(r->spec_batch, spec, N, r->ctfk, S, r->defocus[3 * index + 2], for_fp,
+                            cf.phase_flip_only, cf.wiener_noise_level, beta, r->stream), "CTF slab chain");
+    if ((rc = rec_fft_many(r, cnt, false))) return rc;
+    ESB_CK(launch_square_to_image_many(r->sq_batch, sq, cnt, N, r->squareShift, 1.0f / ((float)N * (float)N), W, H,
+                                       out ? out + (size_t)c0 * img : nullptr, img, accum, crop_out, cut, dim, p_out,
+                                       transpose_out, r->stream), "CTF slab chain");
+  }
+  return ESB_OK;
+}
+
 // Wiener-filtered slab images of prepared projection `index` for the
 // sub-volume paths, into slab_imgs (transposed). The reference pads,
 // transforms, filters and transforms back the same projection once per slab
@@ -701,18 +795,8 @@ static int rec_subvol_slab_images(esb_reconstructor* r, const esb_vol_geom* full
   int rc;
   if ((rc = rec_slab_table(r, full_vol, index, T))) return rc;
   if ((rc = rec_slab_capacity(r, T.count))) return rc;
-  const int want = std::min(T.count, ESB_CTF_SLAB_BATCH);
-  const size_t spec = (size_t)(N / 2 + 1) * N * 2, sq = (size_t)N * N;
-  if (want > r->batch_slabs) {
-    ESB_CK(cudaStreamSynchronize(r->stream), "CTF slab images");
-    cudaFree(r->spec_batch);
-    cudaFree(r->sq_batch);
-    r->spec_batch = r->sq_batch = nullptr;
-    r->batch_slabs = 0;
-    ESB_CK(cudaMalloc(&r->spec_batch, (size_t)want * spec * sizeof(float)), "CTF slab images");
-    ESB_CK(cudaMalloc(&r->sq_batch, (size_t)want * sq * sizeof(float)), "CTF slab images");
-    r->batch_slabs = want;
-  }
+  if ((rc = rec_batch_buffers(r, std::min(T.count, ESB_CTF_SLAB_BATCH)))) return rc;
+  const size_t spec = (size_t)(N / 2 + 1) * N * 2;
   static const int none[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const size_t img = (size_t)W * H;
   PhaseScope ps(r, 2);
@@ -730,15 +814,7 @@ static int rec_subvol_slab_images(esb_reconstructor* r, const esb_vol_geom* full
                           cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &S.d0[j], &S.d1[j]);
     ESB_CK(launch_ctf_slabs(r->fft_d, r->spec_batch, spec, N, r->ctfk, S, r->defocus[3 * index + 2], 0,
                             cf.phase_flip_only, cf.wiener_noise_level, beta, r->stream), "CTF slab images");
-    if (!r->c2r_many_ok[cnt]) {
-      int dims[2] = {N, N};
-      ESB_FFT(cufftPlanMany(&r->c2r_many[cnt], 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, cnt),
-              "CTF slab images plan");
-      r->c2r_many_ok[cnt] = true;
-      ESB_FFT(cufftSetStream(r->c2r_many[cnt], r->stream), "CTF slab images plan");
-    }
-    ESB_FFT(cufftExecC2R(r->c2r_many[cnt], (cufftComplex*)r->spec_batch, (cufftReal*)r->sq_batch),
-            "CTF slab images C2R");
+    if ((rc = rec_fft_many(r, cnt, false))) return rc;
     ESB_CK(launch_square_to_image_batch(r->sq_batch, cnt, N, r->squareShift, 1.0f / ((float)N * (float)N), W, H, W,
                                         r->slab_imgs + (size_t)c0 * img, img, 1, r->stream), "CTF slab images");
   }
@@ -815,14 +891,8 @@ int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, con
       ESB_CK(launch_slicer_fused(c, vol, voxel_type, r->slab_imgs, img, W, T, 0, 0, W, H, r->stream),
              "esb_rec_forward_projection");
     }
-    for (int k = 0; k < T.count; ++k) {
-      float dmin, dmax;
-      esb_defocus_min_max(T.bound[k], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
-                          cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
-                          cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
-      if ((rc = rec_ctf_chain(r, r->slab_imgs + k * img, 1, full, index, dmin, dmax, 1, nullptr, r->proj_d, 1, full)))
-        return rc;
-    }
+    // each slab image through the CTF, added to proj_d in slab order
+    if ((rc = rec_ctf_chain_slabs(r, T, index, r->slab_imgs, 0, 1, full, 1, nullptr, r->proj_d, 1, full, 0))) return rc;
   }
   for (float ray = t_in; cf.variant != ESB_VARIANT_FAST && ray < t_out; ray += step) {
     float dmin, dmax;
@@ -914,20 +984,14 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
     SlabTable T;
     if ((rc = rec_slab_table(r, vg, index, T))) return rc;
     if ((rc = rec_slab_capacity(r, T.count))) return rc;
-    const size_t npx = (size_t)W * H;
-    for (int k = 0; k < T.count; ++k) {
-      float dmin, dmax;
-      esb_defocus_min_max(T.bound[k], r->defocus[3 * index], r->defocus[3 * index + 1], r->tilt[index],
-                          cf.add_tilt_angle, cf.pixel_size_nm, cf.ctf_slice_thickness_nm, cf.volume_shift[2],
-                          cf.ignore_z_shift_for_ctf, cf.switch_ctf_direction, &dmin, &dmax);
-      // cropBorder(proj_d) is re-applied to the residual on every slab (:954)
-      if ((rc = rec_ctf_chain(r, img, 1, p, index, dmin, dmax, 0, r->slab_imgs + k * npx, nullptr, 1, p, 1))) return rc;
-    }
+    // cropBorder(proj_d) is re-applied to the residual on every slab (:954)
+    if ((rc = rec_ctf_chain_slabs(r, T, index, img, 1, 1, p, 0, r->slab_imgs, nullptr, 1, p, 1))) return rc;
     PhaseScope ps(r, 1);
     size_t up_stride = 0;
     const float* up = rec_upsample(r, c, T.count, 1, up_stride);
     ESB_CK(cudaGetLastError(), "back projection");
-    ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, npx, T, W, H, W, lambda, cf.oversampling, 0.f, 0.f,
+    ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, (size_t)W * H, T, W, H, W, lambda, cf.oversampling,
+                                0.f, 0.f,
                                 1, r->stream, 1, up, up_stride), "back projection");
     return ESB_OK;
   }

@@ -157,6 +157,123 @@ __global__ void k_square_to_image_batch(const float* __restrict__ sq, size_t sq_
   out[blockIdx.z * out_stride + (transpose_out ? (size_t)x * ph + y : (size_t)y * pitchE + x)] = v;
 }
 
+// k_crop_to_square for `count` slab inputs at once (square blockIdx.z).
+// seq_crop = 0: input k is images[k] (stride img_stride), cropped in place
+// when apply_crop. seq_crop = 1: every input is the one image `images`,
+// cropped again for each slab, as the reference re-applies cropBorder to the
+// residual before every slab (Reconstructor.cpp:954): input k is the image
+// cropped k + 1 times (from `first` = slabs already applied), and the image
+// is left cropped count more times.
+__global__ void k_crop_to_square_batch(int pw, int ph, float* __restrict__ images, size_t img_stride, int count,
+                                       int apply_crop, int seq_crop, float2 cut, float2 dim, int2 p1, int2 p2, int2 p3,
+                                       int2 p4, int maxsize, float* __restrict__ sq, size_t sq_stride, int bx,
+                                       int by) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= maxsize || y >= maxsize) return;
+  const int xi = x - bx, yi = y - by;
+  const bool inside = xi >= 0 && xi < pw && yi >= 0 && yi < ph;
+  if (!seq_crop) {
+    for (int k = blockIdx.z; k < count; k += gridDim.z) {
+      float val = 0.f;
+      if (inside) {
+        float* img = images + (size_t)k * img_stride;
+        const size_t i = (size_t)yi * pw + xi;
+        val = img[i];
+        if (apply_crop) {
+          val = crop_factor(pw, ph, xi, yi, cut, dim, p1, p2, p3, p4) * val;
+          img[i] = val;
+        }
+      }
+      sq[(size_t)k * sq_stride + (size_t)y * maxsize + x] = val;
+    }
+    return;
+  }
+  if (blockIdx.z != 0) return;
+  float val = 0.f, f = 1.f;
+  size_t i = 0;
+  if (inside) {
+    i = (size_t)yi * pw + xi;
+    val = images[i];
+    f = crop_factor(pw, ph, xi, yi, cut, dim, p1, p2, p3, p4);
+  }
+  for (int k = 0; k < count; ++k) {
+    if (inside) val = f * val;
+    sq[(size_t)k * sq_stride + (size_t)y * maxsize + x] = val;
+  }
+  if (inside) images[i] = val;
+}
+
+// The `ctf` kernel on `count` spectra in place, spectrum k with the defocus
+// range of slab k (same expressions as k_ctf).
+__global__ void k_ctf_batch(float2* __restrict__ spec, size_t spec_stride, int n, CtfConst k, CtfSlabs slabs,
+                            float angle, int applyForFP, int phaseFlipOnly, float wiener, float4 beta) {
+  const unsigned x = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= (unsigned)(n / 2 + 1) || y >= (unsigned)n) return;
+  const float PI = 3.14159265358979323846f;
+  float xpos = (float)x, ypos = (float)y;
+  if (ypos > k.pixelcount * 0.5f) ypos = (k.pixelcount - ypos) * -1.0f;
+  float alpha = (xpos == 0.f) ? (PI * 0.5f) : atan2f(ypos, xpos);
+  float beta_ = alpha - angle;
+  const float c2 = (1.f - cosf(2.f * beta_));
+  float radius = sqrtf(xpos * xpos + ypos * ypos);
+  float length = radius * k.freqStep;
+  float L = k.lambda;
+  const float l = length / 100000000.0f;
+  const float e0 = expf(-beta.y * l - beta.z * l * l - beta.w * l * l * l);
+  const size_t i = (size_t)y * (n / 2 + 1) + x;
+  for (int s = 0; s < slabs.count; ++s) {
+    const float d0 = slabs.d0[s], d1 = slabs.d1[s];
+    float defocus = d0 + c2 * (d1 - d0);
+    float m = (PI / 2.0f) * (k.cs * L * L * L * length * length * length * length - 2.f * defocus * L * length * length);
+    float nn = k.phaseC * sinf(m) + k.ampC * cosf(m);
+    float2 res = spec[(size_t)s * spec_stride + i];
+    if (applyForFP && radius > beta.x && !phaseFlipOnly) {
+      float e = fmaxf(e0, 0.01f);
+      float val = nn * e;
+      if (fabsf(val) < 0.0001f && val >= 0.f) val = 0.0001f;
+      if (fabsf(val) < 0.0001f && val < 0.f) val = -0.0001f;
+      res.x = res.x * -val;
+      res.y = res.y * -val;
+    }
+    if (!applyForFP && radius > beta.x && !phaseFlipOnly) {
+      float e = fmaxf(e0, wiener);
+      float val = nn * e;
+      float f = -val / (val * val + wiener);
+      res.x = res.x * f;
+      res.y = res.y * f;
+    }
+    if (phaseFlipOnly && nn >= 0.f) {
+      res.x = -res.x;
+      res.y = -res.y;
+    }
+    spec[(size_t)s * spec_stride + i] = res;
+  }
+}
+
+// k_square_to_image for `count` squares: scale by inv_norm, crop, and either
+// write image k (transposed or not) or add the squares to `accum` one after
+// the other in slab order (the reference's per-slab accumulation).
+__global__ void k_square_to_image_many(const float* __restrict__ sq, size_t sq_stride, int count, int maxsize,
+                                       size_t shift, float inv_norm, int pw, int ph, float* __restrict__ out,
+                                       size_t out_stride, float* __restrict__ accum, int apply_crop, float2 cut,
+                                       float2 dim, int2 p1, int2 p2, int2 p3, int2 p4, int transpose_out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= pw || y >= ph) return;
+  const float f = apply_crop ? crop_factor(pw, ph, x, y, cut, dim, p1, p2, p3, p4) : 1.f;
+  const size_t i = (size_t)y * pw + x;
+  float a = accum ? accum[i] : 0.f;
+  for (int k = 0; k < count; ++k) {
+    float v = sq[(size_t)k * sq_stride + shift + (size_t)y * maxsize + x] * inv_norm;
+    if (apply_crop) v = f * v;
+    if (out) out[(size_t)k * out_stride + (transpose_out ? (size_t)x * ph + y : i)] = v;
+    if (accum) a += v;
+  }
+  if (accum) accum[i] = a;
+}
+
 // out[x][y] = in[y][x] for a W x H image (32x32 tiles through shared memory).
 __global__ void k_transpose(const float* __restrict__ in, int w, int h, size_t pitchE, float* __restrict__ out) {
   __shared__ float tile[32][33];
@@ -495,6 +612,48 @@ cudaError_t launch_square_to_image_batch(const float* sq, int count, int maxsize
                                               shift, inv_norm, pw, ph, pitchE, out + (size_t)c0 * out_stride,
                                               out_stride, transpose_out); ESB_COUNT_LAUNCH();
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crop_to_square_batch(int pw, int ph, float* images, size_t img_stride, int count, int apply_crop,
+                                        int seq_crop, float2 cut, float2 dim, const int* p, int maxsize, float* sq,
+                                        size_t sq_stride, int bx, int by, cudaStream_t st) {
+  dim3 b(32, 8);
+  dim3 g = grid2(maxsize, maxsize, b);
+  g.z = seq_crop ? 1 : (unsigned)(count < 65535 ? count : 65535);
+  k_crop_to_square_batch<<<g, b, 0, st>>>(pw, ph, images, img_stride, count, apply_crop, seq_crop, cut, dim,
+                                          make_int2(p[0], p[1]), make_int2(p[2], p[3]), make_int2(p[4], p[5]),
+                                          make_int2(p[6], p[7]), maxsize, sq, sq_stride, bx, by);
+  ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ctf_batch(float* spec, size_t spec_stride, int n, const CtfConst& k, const CtfSlabs& slabs_nm,
+                             float angle_deg, int applyForFP, int phaseFlip, float wiener, float4 beta,
+                             cudaStream_t st) {
+  dim3 b(32, 8);
+  CtfSlabs sl = slabs_nm;
+  for (int i = 0; i < sl.count; ++i) {
+    sl.d0[i] = slabs_nm.d0[i] * 0.000000001f;
+    sl.d1[i] = slabs_nm.d1[i] * 0.000000001f;
+  }
+  float ang = angle_deg / 180.0f * 3.14159265358979323846f;
+  k_ctf_batch<<<grid2(n / 2 + 1, n, b), b, 0, st>>>((float2*)spec, spec_stride / 2, n, k, sl, ang, applyForFP,
+                                                    phaseFlip, wiener, beta);
+  ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_square_to_image_many(const float* sq, size_t sq_stride, int count, int maxsize, size_t shift,
+                                        float inv_norm, int pw, int ph, float* out, size_t out_stride, float* accum,
+                                        int apply_crop, float2 cut, float2 dim, const int* p, int transpose_out,
+                                        cudaStream_t st) {
+  dim3 b(32, 8);
+  k_square_to_image_many<<<grid2(pw, ph, b), b, 0, st>>>(sq, sq_stride, count, maxsize, shift, inv_norm, pw, ph, out,
+                                                         out_stride, accum, apply_crop, cut, dim,
+                                                         make_int2(p[0], p[1]), make_int2(p[2], p[3]),
+                                                         make_int2(p[4], p[5]), make_int2(p[6], p[7]), transpose_out);
+  ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
