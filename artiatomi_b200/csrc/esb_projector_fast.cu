@@ -133,93 +133,116 @@ __device__ float cell_sum(const Cell<VT>& C, float qx, float qy, float qz, float
 // cell_sum for a ray whose y coordinate stays in one interpolation cell with
 // a constant weight b (single-axis tilt about y: n.y is 0 or ~1e-10): the
 // trilinear interpolant is a bilinear one in (x, z) of the y-interpolated
-// corners, walked with a 2-D DDA.
+// corners.
+//
+// The walk goes layer by layer along the major axis (z or x, the one with the
+// larger per-sample step). A layer holds at most one crossing of the minor
+// axis, so every step sums two cells, the second empty when the ray does not
+// cross in that layer, and the loop has no data-dependent branches: lanes
+// whose rays cross in different layers stay converged. Both axes are
+// mirrored so that the walk advances in the + direction of each.
+//
+// A cell's M samples have local coordinates (a0 + m da, c0 + m dc); with
+// their mean (a, c) and the bilinear f = e00 + k1 a + k3 c + k5 a c,
+//   sum_m f = M [f(a, c) + k5 da dc (M^2 - 1) / 12].
+// Samples are assigned to cells exactly as by the cell-by-cell DDA (the
+// sample parameter of each face crossing, rounded up).
+template <int VT, bool ZMAJ>
+__device__ float layer_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float qz, float dqx, float dqz, int j0,
+                              int J) {
+  if (j0 >= J) return 0.0f;
+  // major axis m (layers), minor axis n
+  const float qm = ZMAJ ? qz : qx, dqm = ZMAJ ? dqz : dqx;
+  const float qn = ZMAJ ? qx : qz, dqn = ZMAJ ? dqx : dqz;
+  const int sm = dqm < 0.f ? -1 : 1, sn = dqn < 0.f ? -1 : 1;
+  const float Mq = sm > 0 ? qm : -qm, dM = fabsf(dqm);
+  const float Nq = sn > 0 ? qn : -qn, dN = fabsf(dqn);
+  const float fj0 = (float)j0;
+  const float pM = __fmaf_rn(fj0, dM, Mq), pN = __fmaf_rn(fj0, dN, Nq);
+  float fcm = floorf(pM), fcn = floorf(pN);
+  const float inf = FLT_MAX;
+  const float isM = 1.0f / dM;  // dM > 0: the ray moves in x-z, and the major step is the larger one
+  const float isN = dN > 0.f ? 1.0f / dN : inf;
+  float nMs = ((fcm + 1.f) - pM) * isM;
+  float nNs = dN > 0.f ? ((fcn + 1.f) - pN) * isN : inf;
+  const float g = dN * dM * (1.0f / 12.0f);
+  const float jb = fj0 - 0.5f;
+  // 32-bit element offsets (volumes of up to 2^32 voxels; the launchers check)
+  const unsigned SM = ZMAJ ? (unsigned)C.sz : 1u, SN = ZMAJ ? 1u : (unsigned)C.sz;
+  const int nMax = ZMAJ ? C.nz - 1 : C.nx - 1, nNax = ZMAJ ? C.nx - 1 : C.nz - 1;
+  auto clampM = [&](int i) { return (unsigned)(i < 0 ? 0 : (i > nMax ? nMax : i)) * SM; };
+  auto clampN = [&](int i) { return (unsigned)(i < 0 ? 0 : (i > nNax ? nNax : i)) * SN; };
+  const unsigned y0 = (unsigned)(iy < 0 ? 0 : (iy > C.ny - 1 ? C.ny - 1 : iy)) * (unsigned)C.sy;
+  const unsigned y1 = (unsigned)(iy + 1 < 0 ? 0 : (iy + 1 > C.ny - 1 ? C.ny - 1 : iy + 1)) * (unsigned)C.sy;
+  const float ib = 1.0f - b;
+  auto ey = [&](unsigned o) {
+    return ib * Voxel<VT>::load(C.vol, (long)(o + y0)) + b * Voxel<VT>::load(C.vol, (long)(o + y1));
+  };
+  // original indices of the current cell's near and far corners per axis
+  int inF = sn * (int)fcn + sn;
+  int imF = sm * (int)fcm + sm;
+  unsigned on = clampN(inF - sn), of = clampN(inF);
+  unsigned omn = clampM(imF - sm), omf = clampM(imF);
+  float enn = ey(on + omn), efn = ey(of + omn);
+  const float Mt = (float)(J - j0);
+  float fm0 = 0.0f, acc = 0.0f;
+#pragma unroll 1
+  for (int guard = 0; guard < 1 << 20; ++guard) {
+    // samples [fm0, fmA) lie in cell (n, m), [fmA, fmL) in cell (n + 1, m)
+    const float fmL = nMs >= Mt ? Mt : ceilf(nMs);
+    const bool X = nNs <= nMs;
+    const float sA = fminf(nNs, nMs);
+    const float fmA = fmaxf(sA >= Mt ? Mt : ceilf(sA), fm0);
+    const int inF2 = inF + sn;
+    const unsigned o2 = clampN(inF2);
+    const float enf = ey(on + omf), eff = ey(of + omf);
+    float e2n = 0.f, e2f = 0.f;
+    if (X) {
+      e2n = ey(o2 + omn);
+      e2f = ey(o2 + omf);
+    }
+    {
+      const float M = fmA - fm0;
+      const float jm = __fmaf_rn(0.5f, fm0 + fmA, jb);
+      const float a = __fmaf_rn(jm, dN, Nq) - fcn, c = __fmaf_rn(jm, dM, Mq) - fcm;
+      const float k1 = efn - enn, k3 = enf - enn, k5 = (eff - enf) - k1;
+      const float f = fmaf(c, fmaf(a, k5, k3), fmaf(a, k1, enn));
+      acc = fmaf(M, fmaf(k5, fmaf(M * M, g, -g), f), acc);
+    }
+    {
+      const float M = fmL - fmA;
+      const float jm = __fmaf_rn(0.5f, fmA + fmL, jb);
+      const float a = __fmaf_rn(jm, dN, Nq) - (fcn + 1.f), c = __fmaf_rn(jm, dM, Mq) - fcm;
+      const float k1 = e2n - efn, k3 = eff - efn, k5 = (e2f - eff) - k1;
+      const float f = fmaf(c, fmaf(a, k5, k3), fmaf(a, k1, efn));
+      acc = fmaf(M, fmaf(k5, fmaf(M * M, g, -g), f), acc);
+    }
+    fm0 = fmL;
+    if (fm0 >= Mt) break;
+    // next layer, one minor cell further when this layer crossed
+    enn = X ? eff : enf;
+    efn = X ? e2f : eff;
+    if (X) {
+      fcn += 1.f;
+      inF = inF2;
+      on = of;
+      of = o2;
+      nNs = ((fcn + 1.f) - pN) * isN;
+    }
+    fcm += 1.f;
+    imF += sm;
+    omn = omf;
+    omf = clampM(imF);
+    nMs = ((fcm + 1.f) - pM) * isM;
+  }
+  return acc;
+}
+
 template <int VT>
 __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float qz, float dqx, float dqz, int j0,
                              int J) {
-  if (j0 >= J) return 0.0f;
-  const float px = qpos(qx, j0, dqx), pz = qpos(qz, j0, dqz);
-  const float fx = floorf(px), fz = floorf(pz);
-  int ix = (int)fx, iz = (int)fz;
-  const float inf = FLT_MAX;
-  const float isx = dqx != 0.f ? 1.0f / fabsf(dqx) : inf;
-  const float isz = dqz != 0.f ? 1.0f / fabsf(dqz) : inf;
-  float nxs = dqx > 0.f ? (fx + 1.f - px) * isx : (dqx < 0.f ? (px - fx) * isx : inf);
-  float nzs = dqz > 0.f ? (fz + 1.f - pz) * isz : (dqz < 0.f ? (pz - fz) * isz : inf);
-  const int stx = dqx > 0.f ? 1 : -1, stz = dqz > 0.f ? 1 : -1;
-  const float ib = 1.0f - b;
-  // Corner reads without per-load clamping or 64-bit index arithmetic: the
-  // clamped x columns and z rows of the current cell are kept (each step
-  // clamps only the one new index), and element offsets are 32-bit (volumes
-  // of up to 2^32 voxels; launch_project_fast checks).
-  const unsigned sz = (unsigned)C.sz;
-  const unsigned y0 = (unsigned)(iy < 0 ? 0 : (iy > C.ny - 1 ? C.ny - 1 : iy)) * (unsigned)C.sy;
-  const unsigned y1 = (unsigned)(iy + 1 < 0 ? 0 : (iy + 1 > C.ny - 1 ? C.ny - 1 : iy + 1)) * (unsigned)C.sy;
-  auto clampx = [&](int x) { return (unsigned)(x < 0 ? 0 : (x > C.nx - 1 ? C.nx - 1 : x)); };
-  auto clampz = [&](int z) { return (unsigned)(z < 0 ? 0 : (z > C.nz - 1 ? C.nz - 1 : z)) * sz; };
-  auto ey = [&](unsigned xo, unsigned zo) {
-    return ib * Voxel<VT>::load(C.vol, (long)(zo + y0 + xo)) + b * Voxel<VT>::load(C.vol, (long)(zo + y1 + xo));
-  };
-  unsigned x0 = clampx(ix), x1 = clampx(ix + 1), z0 = clampz(iz), z1 = clampz(iz + 1);
-  float e00 = ey(x0, z0), e10 = ey(x1, z0), e01 = ey(x0, z1), e11 = ey(x1, z1);
-  // Integer counters that feed float arithmetic are kept as floats as well
-  // (exact: all values are below 2^24), so the loop converts nothing.
-  const float Mt = (float)(J - j0);
-  const float fj0 = (float)j0;
-  float fm0 = 0.0f;
-  float fix = (float)ix, fiz = (float)iz;
-  const float fstx = (float)stx, fstz = (float)stz;
-  float acc = 0.0f;
-#pragma unroll 1
-  for (int guard = 0; guard < 1 << 20; ++guard) {
-    const float sexit = fminf(nxs, nzs);
-    const float fm1 = (sexit >= Mt) ? Mt : ceilf(sexit);
-    if (fm1 > fm0) {
-      const float a0 = __fsub_rn(__fmaf_rn(fj0 + fm0, dqx, qx), fix);
-      const float c0 = __fsub_rn(__fmaf_rn(fj0 + fm0, dqz, qz), fiz);
-      const float M = fm1 - fm0;
-      const float S1 = 0.5f * M * (M - 1.f);
-      const float S2 = S1 * (2.f * M - 1.f) * (1.f / 3.f);
-      const float k1 = e10 - e00, k3 = e01 - e00, k5 = e11 - e10 - e01 + e00;
-      const float sa = M * a0 + S1 * dqx, sc = M * c0 + S1 * dqz;
-      const float sac = M * a0 * c0 + S1 * (a0 * dqz + c0 * dqx) + S2 * dqx * dqz;
-      acc += e00 * M + k1 * sa + k3 * sc + k5 * sac;
-      fm0 = fm1;
-    }
-    if (fm0 >= Mt) break;
-    if (nxs <= nzs) {
-      ix += stx;
-      fix += fstx;
-      nxs = stx > 0 ? ((fix + 1.0f) - px) * isx : (px - fix) * isx;
-      if (stx > 0) {
-        x0 = x1;
-        x1 = clampx(ix + 1);
-        e00 = e10; e01 = e11;
-        e10 = ey(x1, z0); e11 = ey(x1, z1);
-      } else {
-        x1 = x0;
-        x0 = clampx(ix);
-        e10 = e00; e11 = e01;
-        e00 = ey(x0, z0); e01 = ey(x0, z1);
-      }
-    } else {
-      iz += stz;
-      fiz += fstz;
-      nzs = stz > 0 ? ((fiz + 1.0f) - pz) * isz : (pz - fiz) * isz;
-      if (stz > 0) {
-        z0 = z1;
-        z1 = clampz(iz + 1);
-        e00 = e01; e10 = e11;
-        e01 = ey(x0, z1); e11 = ey(x1, z1);
-      } else {
-        z1 = z0;
-        z0 = clampz(iz);
-        e01 = e00; e11 = e10;
-        e00 = ey(x0, z0); e10 = ey(x1, z0);
-      }
-    }
-  }
-  return acc;
+  if (fabsf(dqz) >= fabsf(dqx)) return layer_sum_xz<VT, true>(C, qx, b, iy, qz, dqx, dqz, j0, J);
+  return layer_sum_xz<VT, false>(C, qx, b, iy, qz, dqx, dqz, j0, J);
 }
 
 // Sum over the samples of one sub-ray from t0 to tout (first_at_source: the
