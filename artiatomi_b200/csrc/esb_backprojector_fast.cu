@@ -78,6 +78,131 @@ __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __res
   }
 }
 
+// Geometry of k_bp_axis: single-axis tilt (n.y = 0), power-of-two
+// oversampling, no anisotropy, pre-sampled images.
+struct AxisGeom {
+  float3 U, V;     // detector coordinate of a world point: u = U.p + U0, v = V.p + V0
+  float U0, V0;
+  float hu, hv;    // half shadow extents in pixels (as BpGeom)
+  float wu, wv;    // in-plane offset of a sample perpendicular to n in x-z, per pixel of u and v
+  float yu, yv;    // its y component per pixel of u and v
+  float hby;       // half voxel size in y
+  float L0, w1K, K;  // chord trapezoid: L(w) = min(L0, max(0, w1K - |w| K))
+};
+
+// Depth of the macro cell's first corner (macro_footprint's corner 0, the
+// reference's expression), which selects the quad's CTF slab.
+__device__ __forceinline__ float macro_depth(const KConst& k, int x, int y, int z) {
+  const float mnx = fadd(k.bbMin.x, fmul((float)x, k.vs.x)), mny = fadd(k.bbMin.y, fmul((float)y, k.vs.y)),
+              mnz = fadd(k.bbMin.z, fmul((float)z, k.vs.z));
+  const float ndet = fadd(fadd(fmul(-k.n.x, k.det.x), -fmul(k.n.y, k.det.y)), -fmul(k.n.z, k.det.z));
+  const float t = fadd(fadd(fmul(k.n.x, mnx), fmul(k.n.y, mny)), fmul(k.n.z, mnz));
+  return fabsf(fadd(t, ndet));
+}
+
+// k_bp_fast for single-axis tilt series on pre-sampled images. With n.y = 0
+// the chord of a sample's ray through a voxel depends only on the ray's
+// offset w from the voxel centre perpendicular to n in the x-z plane (a
+// trapezoid: the plateau min(2 hx / |n.x|, 2 hz / |n.z|), falling linearly to
+// 0 at |w| = hx |n.z| + hz |n.x| with slope 1 / (|n.x| |n.z|)), cut to 0 when
+// the offset's y component leaves the voxel. Samples are the sub-pixel grid
+// points (m + 0.5) / os inside the voxel's shadow and inside
+// [0, pw - 1) x [0, ph - 1), as the clamped macro-cell rectangle allows.
+template <int VT>
+__global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __restrict__ vol, SlabTable slabs,
+                                                 int pw, int ph, float lambda, int os, float inv, float distMin,
+                                                 float distMax, const float* __restrict__ ups, size_t up_stride) {
+  const int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int z = (int)blockIdx.z;
+  const int ny = (int)k.dim.y, nz = (int)k.dim.z;
+  if (q >= k.dimXQuarter || y >= ny || z >= nz) return;
+  const int x = 4 * q;
+  const float depth = macro_depth(k, x, y, z);
+  const float* up = ups;
+  if (slabs.count > 0) {
+    if (!(depth >= slabs.bound[0] && depth < slabs.bound[slabs.count])) return;
+    int s = 0;
+    while (s + 1 < slabs.count && depth >= slabs.bound[s + 1]) ++s;
+    up += (size_t)s * up_stride;
+  } else if (!(depth >= distMin && depth < distMax)) {
+    return;
+  }
+  const int upH = ph * os;
+  const float fos = (float)os;
+  const int mu_max = (pw - 1) * os - 1, mv_max = (ph - 1) * os - 1;
+  const float cy = k.bbMin.y + ((float)y + 0.5f) * k.vs.y, cz = k.bbMin.z + ((float)z + 0.5f) * k.vs.z;
+  const float uyz = g.U.y * cy + g.U.z * cz + g.U0, vyz = g.V.y * cy + g.V.z * cz + g.V0;
+  const float dwv = inv * g.wv, dyv = inv * g.yv;
+  const long base = ((long)z * ny + y) * (long)k.dim.x + x;
+  float res[4], has[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float cx = k.bbMin.x + ((float)(x + i) + 0.5f) * k.vs.x;
+    const float uc = g.U.x * cx + uyz, vc = g.V.x * cx + vyz;
+    const int mu0 = max((int)ceilf((uc - g.hu) * fos - 0.5f), 0);
+    const int mu1 = min((int)floorf((uc + g.hu) * fos - 0.5f), mu_max);
+    const int mv0 = max((int)ceilf((vc - g.hv) * fos - 0.5f), 0);
+    const int mv1 = min((int)floorf((vc + g.hv) * fos - 0.5f), mv_max);
+    const float dv0 = ((float)mv0 + 0.5f) * inv - vc;
+    float a = 0.f, da = 0.f;
+#pragma unroll 1
+    for (int mu = mu0; mu <= mu1; ++mu) {
+      const float du = ((float)mu + 0.5f) * inv - uc;
+      float w = du * g.wu + dv0 * g.wv, dy = du * g.yu + dv0 * g.yv;
+      const float* p = up + (size_t)mu * upH + mv0;
+#pragma unroll 1
+      for (int mv = mv0; mv <= mv1; ++mv) {
+        float L = fminf(g.L0, fmaxf(0.f, fmaf(-fabsf(w), g.K, g.w1K)));
+        L = fabsf(dy) <= g.hby ? L : 0.f;
+        a = fmaf(__ldg(p), L, a);
+        da += L;
+        w += dwv;
+        dy += dyv;
+        ++p;
+      }
+    }
+    res[i] = a;
+    has[i] = da;
+  }
+  if (VT == ESB_VOXEL_F32 && (((uintptr_t)((float*)vol + base)) & 15) == 0) {
+    float4 v = *((float4*)((float*)vol + base));
+    if (has[0] > 0.f) v.x += lambda * res[0] / has[0];
+    if (has[1] > 0.f) v.y += lambda * res[1] / has[1];
+    if (has[2] > 0.f) v.z += lambda * res[2] / has[2];
+    if (has[3] > 0.f) v.w += lambda * res[3] / has[3];
+    *((float4*)((float*)vol + base)) = v;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      if (has[i] > 0.f) Voxel<VT>::store(vol, base + i, Voxel<VT>::loadrw(vol, base + i) + lambda * res[i] / has[i]);
+    }
+  }
+}
+
+AxisGeom make_axis_geom(const KConst& k, const BpGeom& b) {
+  AxisGeom g;
+  g.U = b.U;
+  g.V = b.V;
+  g.U0 = b.U0;
+  g.V0 = b.V0;
+  g.hu = b.hu;
+  g.hv = b.hv;
+  // offset d = du * u + dv * v; w = d.x n.z - d.z n.x
+  g.wu = k.u.x * k.n.z - k.u.z * k.n.x;
+  g.wv = k.v.x * k.n.z - k.v.z * k.n.x;
+  g.yu = k.u.y;
+  g.yv = k.v.y;
+  g.hby = b.hb.y;
+  const float anx = fabsf(k.n.x), anz = fabsf(k.n.z);
+  const float hx = b.hb.x, hz = b.hb.z;
+  g.L0 = fminf(anx > 0.f ? 2.f * hx / anx : FLT_MAX, anz > 0.f ? 2.f * hz / anz : FLT_MAX);
+  const float prod = anx * anz;
+  g.K = prod > 1e-30f ? 1.0f / prod : 1e30f;
+  g.w1K = (hx * anz + hz * anx) * g.K;
+  return g;
+}
+
 // The slab images (transposed, [x][y], stride img_stride) sampled at every
 // sub-pixel grid point: up[s][mu][mv] = image s at ((mu + 0.5) / os,
 // (mv + 0.5) / os), clamp addressing, nearest or bilinear as the
@@ -106,6 +231,16 @@ cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float
   const BpGeom g = make_geom(k, os);
   const float inv = 1.0f / (float)os;
   dim3 blk(32, 4, 1), grd((nq + 31) / 32, (ny + 3) / 4, nz);
+  if (ups && g.exact_grid && g.aniso_identity && fabsf(k.n.y) <= 1e-6f) {
+    const AxisGeom a = make_axis_geom(k, g);
+    switch (vt) {
+      case ESB_VOXEL_F32: k_bp_axis<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, a, vol, slabs, pw, ph, lambda, os, inv, distMin, distMax, ups, up_stride); break;
+      case ESB_VOXEL_F16: k_bp_axis<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, a, vol, slabs, pw, ph, lambda, os, inv, distMin, distMax, ups, up_stride); break;
+      default: k_bp_axis<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(k, a, vol, slabs, pw, ph, lambda, os, inv, distMin, distMax, ups, up_stride); break;
+    }
+    ESB_COUNT_LAUNCH();
+    return cudaGetLastError();
+  }
   switch (vt) {
     case ESB_VOXEL_F32: k_bp_fast<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed, ups, up_stride); ESB_COUNT_LAUNCH(); break;
     case ESB_VOXEL_F16: k_bp_fast<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, g, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, distMax, linear, transposed, ups, up_stride); ESB_COUNT_LAUNCH(); break;
