@@ -88,6 +88,18 @@ struct AxisGeom {
   float yu, yv;    // its y component per pixel of u and v
   float hby;       // half voxel size in y
   float L0, w1K, K;  // chord trapezoid: L(w) = min(L0, max(0, w1K - |w| K))
+  // macro-cell rectangle of quad (x, y, z), affine in the quad position:
+  // u_lo/hi = ru.w + x ru.x + y ru.y + z ru.z + (ulo, uhi), same for v
+  float4 ru, rv;
+  float ulo, uhi, vlo, vhi;
+  // The rectangle can be smaller than the macro cell's shadow (detector axes
+  // rotated against the volume axes). Its integer bounds (floor / ceil of the
+  // extremes) decide which samples of the clipped band are taken; the affine
+  // extremes agree with the reference's to ~1e-3 pixel, so they give the
+  // same samples unless the band reaches the nearest sub-pixel sample beyond
+  // an integer bound (0.5 / os). Then the rectangle is evaluated per quad
+  // with the reference's expressions (macro_footprint).
+  int clips;
 };
 
 // Depth of the macro cell's first corner (macro_footprint's corner 0, the
@@ -100,14 +112,34 @@ __device__ __forceinline__ float macro_depth(const KConst& k, int x, int y, int 
   return fabsf(fadd(t, ndet));
 }
 
+// The reference's macro-cell rectangle (macro_footprint): the cell's 8
+// corners are projected along n onto the detector plane, the bounding box
+// (lo, hi) of those hit points is taken in world coordinates (x swapped when
+// n.x <= 0) and only lo and hi are mapped to the detector. With the hit point
+// h = A p + b linear in the corner p, lo and hi are affine in the quad
+// position, and so are their detector coordinates; the rectangle is the
+// reference's up to float rounding. It can be smaller than the voxels'
+// shadows when the detector axes are rotated against the volume axes, and
+// then clips samples as the reference does.
+__device__ __forceinline__ void macro_rect(const AxisGeom& g, int x, int y, int z, int pw, int ph, int& pbx, int& pby,
+                                           int& pbz, int& pbw) {
+  const float uL = fmaf((float)z, g.ru.z, fmaf((float)y, g.ru.y, fmaf((float)x, g.ru.x, g.ru.w)));
+  const float vL = fmaf((float)z, g.rv.z, fmaf((float)y, g.rv.y, fmaf((float)x, g.rv.x, g.rv.w)));
+  const float plx = uL + g.ulo, phx = uL + g.uhi, ply = vL + g.vlo, phy = vL + g.vhi;
+  pbx = (int)fminf(fmaxf(floorf(fminf(plx, phx)), 0.0f), (float)(pw - 1));
+  pby = (int)fminf(fmaxf(ceilf(fmaxf(plx, phx)), 0.0f), (float)(pw - 1));
+  pbz = (int)fminf(fmaxf(floorf(fminf(ply, phy)), 0.0f), (float)(ph - 1));
+  pbw = (int)fminf(fmaxf(ceilf(fmaxf(ply, phy)), 0.0f), (float)(ph - 1));
+}
+
 // k_bp_fast for single-axis tilt series on pre-sampled images. With n.y = 0
 // the chord of a sample's ray through a voxel depends only on the ray's
 // offset w from the voxel centre perpendicular to n in the x-z plane (a
 // trapezoid: the plateau min(2 hx / |n.x|, 2 hz / |n.z|), falling linearly to
 // 0 at |w| = hx |n.z| + hz |n.x| with slope 1 / (|n.x| |n.z|)), cut to 0 when
 // the offset's y component leaves the voxel. Samples are the sub-pixel grid
-// points (m + 0.5) / os inside the voxel's shadow and inside
-// [0, pw - 1) x [0, ph - 1), as the clamped macro-cell rectangle allows.
+// points (m + 0.5) / os inside the voxel's shadow and inside the quad's
+// macro-cell rectangle [pbx, pby) x [pbz, pbw) (macro_rect).
 template <int VT>
 __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __restrict__ vol, SlabTable slabs,
                                                  int pw, int ph, float lambda, int os, float inv, float distMin,
@@ -128,9 +160,16 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
   } else if (!(depth >= distMin && depth < distMax)) {
     return;
   }
+  int pbx, pby, pbz, pbw;
+  if (g.clips) {
+    float d;
+    macro_footprint(k, x, y, z, pw, ph, d, pbx, pby, pbz, pbw);
+  } else {
+    macro_rect(g, x, y, z, pw, ph, pbx, pby, pbz, pbw);
+  }
   const int upH = ph * os;
   const float fos = (float)os;
-  const int mu_max = (pw - 1) * os - 1, mv_max = (ph - 1) * os - 1;
+  const int mu_min = pbx * os, mu_max = pby * os - 1, mv_min = pbz * os, mv_max = pbw * os - 1;
   const float cy = k.bbMin.y + ((float)y + 0.5f) * k.vs.y, cz = k.bbMin.z + ((float)z + 0.5f) * k.vs.z;
   const float uyz = g.U.y * cy + g.U.z * cz + g.U0, vyz = g.V.y * cy + g.V.z * cz + g.V0;
   const float dwv = inv * g.wv, dyv = inv * g.yv;
@@ -140,9 +179,9 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
   for (int i = 0; i < 4; ++i) {
     const float cx = k.bbMin.x + ((float)(x + i) + 0.5f) * k.vs.x;
     const float uc = g.U.x * cx + uyz, vc = g.V.x * cx + vyz;
-    const int mu0 = max((int)ceilf((uc - g.hu) * fos - 0.5f), 0);
+    const int mu0 = max((int)ceilf((uc - g.hu) * fos - 0.5f), mu_min);
     const int mu1 = min((int)floorf((uc + g.hu) * fos - 0.5f), mu_max);
-    const int mv0 = max((int)ceilf((vc - g.hv) * fos - 0.5f), 0);
+    const int mv0 = max((int)ceilf((vc - g.hv) * fos - 0.5f), mv_min);
     const int mv1 = min((int)floorf((vc + g.hv) * fos - 0.5f), mv_max);
     const float dv0 = ((float)mv0 + 0.5f) * inv - vc;
     float a = 0.f, da = 0.f;
@@ -180,7 +219,7 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
   }
 }
 
-AxisGeom make_axis_geom(const KConst& k, const BpGeom& b) {
+AxisGeom make_axis_geom(const KConst& k, const BpGeom& b, int os) {
   AxisGeom g;
   g.U = b.U;
   g.V = b.V;
@@ -200,6 +239,73 @@ AxisGeom make_axis_geom(const KConst& k, const BpGeom& b) {
   const float prod = anx * anz;
   g.K = prod > 1e-30f ? 1.0f / prod : 1e30f;
   g.w1K = (hx * anz + hz * anx) * g.K;
+  // macro-cell rectangle: h = A p + b with A = I - sg n n^T, b = -sg ndet n,
+  // sg the sign of n.p + ndet over the volume (the detector lies outside it)
+  const double n[3] = {k.n.x, k.n.y, k.n.z};
+  const double det[3] = {k.det.x, k.det.y, k.det.z};
+  const double ndet = -n[0] * det[0] - n[1] * det[1] - n[2] * det[2];
+  const double bmin[3] = {k.bbMin.x, k.bbMin.y, k.bbMin.z}, vs[3] = {k.vs.x, k.vs.y, k.vs.z};
+  const double ext[3] = {5.0 * vs[0], vs[1], vs[2]};  // the 5 x 1 x 1 macro cell
+  const double dim[3] = {k.dim.x, k.dim.y, k.dim.z};
+  double ctr = ndet;  // n.p + ndet at the volume centre
+  for (int j = 0; j < 3; ++j) ctr += n[j] * (bmin[j] + 0.5 * vs[j] * dim[j]);
+  const double sg = ctr < 0.0 ? -1.0 : 1.0;
+  double A[3][3], base[3], dlo[3], dhi[3];
+  for (int r = 0; r < 3; ++r) {
+    base[r] = -sg * ndet * n[r];
+    dlo[r] = dhi[r] = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      A[r][c] = (r == c ? 1.0 : 0.0) - sg * n[r] * n[c];
+      base[r] += A[r][c] * bmin[c];
+      const double e = A[r][c] * ext[c];
+      dlo[r] += e < 0.0 ? e : 0.0;
+      dhi[r] += e > 0.0 ? e : 0.0;
+    }
+  }
+  if (k.n.x <= 0.0f) {  // the reference swaps lo.x and hi.x
+    const double t = dlo[0];
+    dlo[0] = dhi[0];
+    dhi[0] = t;
+  }
+  const double U[3] = {b.U.x, b.U.y, b.U.z}, V[3] = {b.V.x, b.V.y, b.V.z};
+  double ru[4] = {0, 0, 0, b.U0}, rv[4] = {0, 0, 0, b.V0};
+  double ulo = 0, uhi = 0, vlo = 0, vhi = 0;
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) {
+      ru[c] += U[r] * A[r][c] * vs[c];
+      rv[c] += V[r] * A[r][c] * vs[c];
+    }
+    ru[3] += U[r] * base[r];
+    rv[3] += V[r] * base[r];
+    ulo += U[r] * dlo[r];
+    uhi += U[r] * dhi[r];
+    vlo += V[r] * dlo[r];
+    vhi += V[r] * dhi[r];
+  }
+  // true extent of the macro cell's shadow around the projection of A m:
+  // sum_c min/max(0, (U A)_c ext_c); the rectangle clips when its own
+  // extent (U dlo, U dhi) is narrower
+  double su_lo = 0, su_hi = 0, sv_lo = 0, sv_hi = 0;
+  for (int c = 0; c < 3; ++c) {
+    double ua = 0, va = 0;
+    for (int r = 0; r < 3; ++r) {
+      ua += U[r] * A[r][c];
+      va += V[r] * A[r][c];
+    }
+    su_lo += ua * ext[c] < 0 ? ua * ext[c] : 0;
+    su_hi += ua * ext[c] > 0 ? ua * ext[c] : 0;
+    sv_lo += va * ext[c] < 0 ? va * ext[c] : 0;
+    sv_hi += va * ext[c] > 0 ? va * ext[c] : 0;
+  }
+  const double band = fmax(fmax(fmin(ulo, uhi) - su_lo, su_hi - fmax(ulo, uhi)),
+                           fmax(fmin(vlo, vhi) - sv_lo, sv_hi - fmax(vlo, vhi)));
+  g.clips = band > 0.5 / os - 0.01 ? 1 : 0;
+  g.ru = make_float4((float)ru[0], (float)ru[1], (float)ru[2], (float)ru[3]);
+  g.rv = make_float4((float)rv[0], (float)rv[1], (float)rv[2], (float)rv[3]);
+  g.ulo = (float)ulo;
+  g.uhi = (float)uhi;
+  g.vlo = (float)vlo;
+  g.vhi = (float)vhi;
   return g;
 }
 
@@ -232,7 +338,7 @@ cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float
   const float inv = 1.0f / (float)os;
   dim3 blk(32, 4, 1), grd((nq + 31) / 32, (ny + 3) / 4, nz);
   if (ups && g.exact_grid && g.aniso_identity && fabsf(k.n.y) <= 1e-6f) {
-    const AxisGeom a = make_axis_geom(k, g);
+    const AxisGeom a = make_axis_geom(k, g, os);
     switch (vt) {
       case ESB_VOXEL_F32: k_bp_axis<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(k, a, vol, slabs, pw, ph, lambda, os, inv, distMin, distMax, ups, up_stride); break;
       case ESB_VOXEL_F16: k_bp_axis<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(k, a, vol, slabs, pw, ph, lambda, os, inv, distMin, distMax, ups, up_stride); break;

@@ -79,3 +79,111 @@ def test_more_than_256_ctf_slabs_is_reported():
     rec.reset_projections()
     with pytest.raises(L.EsbError, match="256 CTF slabs"):
         rec.forward_projection(case["vg"], torch.zeros((64, 64, 64), device="cuda"), 1, False)
+
+
+def _rotated_case(psi_deg, tilt_x):
+    """A small case whose tilt axis is rotated in the detector plane by
+    psi_deg (plus jitter) and, with tilt_x != 0, tilted out of the volume's
+    y axis (AddTiltXAngle: the beam gets a y component)."""
+    import artiatomi_b200 as E
+    from oracle import geometry as G
+
+    case = small_case(dims=(48, 48, 24), n_proj=7, W=64, H=64, shift=1.0, psi=0.3)
+    psi = (case["psi"] + np.float32(psi_deg)).astype(np.float32)
+    cfg = dict(add_tilt_x_angle=tilt_x) if tilt_x else {}
+    case["pg"] = E.projection_geometry(E.Markers(case["tilt"], case["xs"], case["ys"], None, psi), 64, 64,
+                                       E.TiltConfig(**cfg))
+    case["og"] = G.projection_geometry(case["tilt"], case["xs"], case["ys"], None, psi, 64, 64, cfg)
+    return case
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("psi_deg,tilt_x", [(37.0, 0.0), (90.0, 0.0), (-61.0, 0.0), (12.0, 0.8)])
+def test_fast_kernels_rotated_and_tilted_axes(psi_deg, tilt_x):
+    """The single-axis kernels (layer walk of the projector, trapezoid chords
+    of the back-projection on pre-sampled images) at large in-plane rotations,
+    and the general 3-D walk / chord kernels under a tilted axis, against the
+    oracle: forward projection, one back-projection of the reconstructor, and
+    SART with CTF."""
+    import torch
+
+    import artiatomi_b200 as E
+    from oracle import driver as D
+    from oracle import geometry as G
+    from oracle.driver import OracleReconstructor
+    from tests.test_parity_recon import _ctf_cfg, _projections
+
+    case = _rotated_case(psi_deg, tilt_x)
+    W, H, n = case["W"], case["H"], len(case["tilt"])
+    vol_d = cuda(case["vol"])
+    for i in range(n):
+        c = E.set_constant_values(case["pg"][i], case["vg"])
+        if tilt_x == 0.0:
+            assert abs(c.proj_norm[1]) <= 1e-6
+        else:
+            assert abs(c.proj_norm[1]) > 1e-3
+        proj = torch.zeros((H, W), device="cuda")
+        dist = torch.zeros((H, W), device="cuda")
+        E.forward_project(c, vol_d, proj, dist, fast=True)
+        po = np.zeros((H, W), np.float32)
+        do = np.zeros((H, W), np.float32)
+        D.fp_march(G.orc_geom(case["og"][i], case["vo"]), case["vol"], 0, W, H, po, do, precision=0)
+        assert rel_l2(host(proj), po) <= 1e-4, (i, rel_l2(host(proj), po))
+    # one back-projection through the reconstructor (pre-sampled images, OS 2)
+    # against the generic per-voxel-shadow kernel on the same cropped image
+    # (both take the reference's FP32 macro-cell rectangle) and the FP64
+    # oracle. At large rotations the rectangle clips the voxels' shadows and
+    # its float rounding decides samples in the clipped band, so the
+    # reference's own FP32 result (oracle precision 0) differs from FP64 by
+    # up to ~1e-2; that difference bounds the agreement with FP64 there.
+    cfgd = dict(lambda_=0.5, oversampling=2, cut_length=(1.0, 1.0), dim_length=(3.0, 3.0))
+    rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **cfgd), case["pg"], case["tilt"])
+    orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], precision=1)
+    rng = np.random.default_rng(8)
+    vol0 = rng.normal(size=case["vol"].shape).astype(np.float32)
+    proj_v, _, _ = rec.views()
+    clipping = abs(psi_deg) % 90.0 > 5.0
+    orc32 = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], precision=0)
+    for i in (0, n // 2, n - 1):
+        img = rng.normal(size=(H, W)).astype(np.float32)
+        v = cuda(vol0)
+        proj_v.copy_(cuda(img))
+        rec.back_projection(case["vg"], v, i, 1.0)
+        cropped = img.copy()
+        D.crop_border(cropped, cfgd["cut_length"], cfgd["dim_length"], G.compute_hit_points(case["og"][i], case["vo"]))
+        vg_ = cuda(vol0)
+        E.back_project(E.set_constant_values(case["pg"][i], case["vg"], for_bp=True), vg_, cuda(cropped), 0.5, 2,
+                       fast=True)
+        e = rel_l2(host(v) - vol0, host(vg_) - vol0)
+        assert e <= 1e-5, (i, e)
+        vo = vol0.copy()
+        orc.back_projection(case["vo"], vo, 0, i, 1.0, img=img.copy())
+        e = rel_l2(host(v) - vol0, vo - vol0)
+        if clipping:
+            v32 = vol0.copy()
+            orc32.back_projection(case["vo"], v32, 0, i, 1.0, img=img.copy())
+            e_ref = rel_l2(v32 - vol0, vo - vol0)
+            assert e <= max(1e-5, 1.5 * e_ref), (i, e, e_ref)
+        else:
+            assert e <= 1e-5, (i, e)
+    # SART with CTF
+    rng = np.random.default_rng(3)
+    dmid = rng.uniform(2800.0, 3200.0, n)
+    defocus = np.stack([dmid - 40.0, dmid + 40.0, rng.uniform(0, 180, n)], 1).astype(np.float32).ravel()
+    projs = _projections(case)
+    il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, case["tilt"])
+    cfgd = dict(_ctf_cfg(max(W, H)), lambda_=0.5, oversampling=2)
+    rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **cfgd), case["pg"], case["tilt"], defocus)
+    v = cuda(np.zeros(case["vol"].shape, np.float32))
+    rec.sart(case["vg"], v, cuda(projs), il, iterations=2, sirt_count=2)
+    orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], defocus, precision=1)
+    ref = np.zeros(case["vol"].shape, np.float32)
+    orc.sart(case["vo"], ref, 0, projs, il, 2, 2)
+    assert np.abs(ref).max() > 0
+    tol = 1e-3
+    if clipping:
+        ref32 = np.zeros(case["vol"].shape, np.float32)
+        OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], defocus, precision=0).sart(case["vo"], ref32, 0,
+                                                                                            projs, il, 2, 2)
+        tol = max(tol, 1.5 * rel_l2(ref32, ref))
+    assert rel_l2(host(v), ref) <= tol, (rel_l2(host(v), ref), tol)
