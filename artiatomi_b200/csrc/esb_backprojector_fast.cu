@@ -190,16 +190,19 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
       const float du = ((float)mu + 0.5f) * inv - uc;
       float w = du * g.wu + dv0 * g.wv, dy = du * g.yu + dv0 * g.yv;
       const float* p = up + (size_t)mu * upH + mv0;
-#pragma unroll 1
-      for (int mv = mv0; mv <= mv1; ++mv) {
-        float L = fminf(g.L0, fmaxf(0.f, fmaf(-fabsf(w), g.K, g.w1K)));
-        L = fabsf(dy) <= g.hby ? L : 0.f;
-        a = fmaf(__ldg(p), L, a);
+      const int cnt = mv1 - mv0 + 1;
+      auto body = [&](int j) {
+        const float ww = fmaf((float)j, dwv, w), yy = fmaf((float)j, dyv, dy);
+        float L = fminf(g.L0, fmaxf(0.f, fmaf(-fabsf(ww), g.K, g.w1K)));
+        L = fabsf(yy) <= g.hby ? L : 0.f;
+        a = fmaf(__ldg(p + j), L, a);
         da += L;
-        w += dwv;
-        dy += dyv;
-        ++p;
-      }
+      };
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < cnt) body(j);
+#pragma unroll 1
+      for (int j = 4; j < cnt; ++j) body(j);
     }
     res[i] = a;
     has[i] = da;

@@ -196,11 +196,7 @@ __device__ float layer_sum_xz(const Cell<VT>& C, float qx, float b, int iy, floa
     const int inF2 = inF + sn;
     const unsigned o2 = clampN(inF2);
     const float enf = ey(on + omf), eff = ey(of + omf);
-    float e2n = 0.f, e2f = 0.f;
-    if (X) {
-      e2n = ey(o2 + omn);
-      e2f = ey(o2 + omf);
-    }
+    const float e2n = ey(o2 + omn), e2f = ey(o2 + omf);
     {
       const float M = fmA - fm0;
       const float jm = __fmaf_rn(0.5f, fm0 + fmA, jb);
