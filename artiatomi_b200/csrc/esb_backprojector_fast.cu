@@ -185,8 +185,10 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
     const int mv1 = min((int)floorf((vc + g.hv) * fos - 0.5f), mv_max);
     const float dv0 = ((float)mv0 + 0.5f) * inv - vc;
     float a = 0.f, da = 0.f;
-#pragma unroll 1
-    for (int mu = mu0; mu <= mu1; ++mu) {
+    // a voxel's shadow holds 2-3 sub-pixel samples per axis at OS 2: the
+    // first rows and samples are unrolled (predicated), any further ones loop
+    const int rows = mu1 - mu0 + 1;
+    auto row = [&](int mu) {
       const float du = ((float)mu + 0.5f) * inv - uc;
       float w = du * g.wu + dv0 * g.wv, dy = du * g.yu + dv0 * g.yv;
       const float* p = up + (size_t)mu * upH + mv0;
@@ -199,25 +201,30 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
         da += L;
       };
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < 3; ++j)
         if (j < cnt) body(j);
 #pragma unroll 1
-      for (int j = 4; j < cnt; ++j) body(j);
-    }
+      for (int j = 3; j < cnt; ++j) body(j);
+    };
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+      if (r < rows) row(mu0 + r);
+#pragma unroll 1
+    for (int r = 2; r < rows; ++r) row(mu0 + r);
     res[i] = a;
     has[i] = da;
   }
   if (VT == ESB_VOXEL_F32 && (((uintptr_t)((float*)vol + base)) & 15) == 0) {
     float4 v = *((float4*)((float*)vol + base));
-    if (has[0] > 0.f) v.x += lambda * res[0] / has[0];
-    if (has[1] > 0.f) v.y += lambda * res[1] / has[1];
-    if (has[2] > 0.f) v.z += lambda * res[2] / has[2];
-    if (has[3] > 0.f) v.w += lambda * res[3] / has[3];
+    if (has[0] > 0.f) v.x += __fdividef(lambda * res[0], has[0]);
+    if (has[1] > 0.f) v.y += __fdividef(lambda * res[1], has[1]);
+    if (has[2] > 0.f) v.z += __fdividef(lambda * res[2], has[2]);
+    if (has[3] > 0.f) v.w += __fdividef(lambda * res[3], has[3]);
     *((float4*)((float*)vol + base)) = v;
   } else {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      if (has[i] > 0.f) Voxel<VT>::store(vol, base + i, Voxel<VT>::loadrw(vol, base + i) + lambda * res[i] / has[i]);
+      if (has[i] > 0.f) Voxel<VT>::store(vol, base + i, Voxel<VT>::loadrw(vol, base + i) + __fdividef(lambda * res[i], has[i]));
     }
   }
 }
