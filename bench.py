@@ -41,12 +41,13 @@ UNIT = "voxel-updates/s"
 
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum,
 # dram__bytes_write.sum) on the 1024x1024x64 volume / 1024^2 detector case,
-# per unit of the roofline: forward projection = k_slicer_fused + k_travlen,
-# back-projection = k_bp_fast. The volume part scales with the voxels, the
-# image part with the pixels.
+# per unit of the roofline: forward projection = k_slicer_fused (volume read,
+# slab images written) + k_travlen (image read), back-projection = k_bp_axis
+# (volume read and written, pre-sampled slab images read). The volume part
+# scales with the voxels, the image part with the pixels.
 DRAM_V, DRAM_P = 1024 * 1024 * 64, 1024 * 1024
-DRAM_FP_READ, DRAM_FP_IMG = 268.74e6, 4.77e6 + 4.20e6
-DRAM_BP_READ, DRAM_BP_WRITE, DRAM_BP_IMG = 274.97e6 - 4.19e6, 207.27e6, 4.19e6
+DRAM_FP_READ, DRAM_FP_IMG = 268.62e6, 4.74e6 + 4.20e6
+DRAM_BP_READ, DRAM_BP_WRITE, DRAM_BP_IMG = 268.44e6, 211.57e6, 292.94e6 - 268.44e6
 
 
 def _peaks():
@@ -341,7 +342,8 @@ def run_esb(args):
                            "projections": params["n_proj"], "projection_size": [params["W"], params["H"]],
                            "oversampling": params["os"], "sirt_count": sirt, "ctf": params["ctf"],
                            "ctf_slab_nm": 30.0, "voxel_storage": "f32", "kernels": args.variant,
-                           "l2": "inputs larger than L2 (volume 1 GiB)", "parallelism": f"replicas x{ws}"},
+                           "l2": f"inputs larger than L2 (volume {wl.voxels * 4 / 2**20:.0f} MiB)",
+                           "parallelism": f"replicas x{ws}"},
                 "e2e": {"value": e2e_value, "unit": UNIT,
                         "h2d_bytes_per_step": int(wl.projections.numel() * 4),
                         "d2h_bytes_per_step": int(vol.numel() * 4)},
