@@ -248,5 +248,219 @@ inline BpGeom make_geom(const KConst& k, int os) {
   return g;
 }
 
+// Geometry of the single-axis back-projection (axis_sums): tilt axis along
+// y (n.y = 0), power-of-two oversampling, no magnification anisotropy.
+struct AxisGeom {
+  float3 U, V;     // detector coordinate of a world point: u = U.p + U0, v = V.p + V0
+  float U0, V0;
+  float hu, hv;    // half shadow extents in pixels (as BpGeom)
+  float wu, wv;    // in-plane offset of a sample perpendicular to n in x-z, per pixel of u and v
+  float yu, yv;    // its y component per pixel of u and v
+  float hby;       // half voxel size in y
+  float L0, w1K, K;  // chord trapezoid: L(w) = min(L0, max(0, w1K - |w| K))
+  // macro-cell rectangle of quad (x, y, z), affine in the quad position:
+  // u_lo/hi = ru.w + x ru.x + y ru.y + z ru.z + (ulo, uhi), same for v
+  float4 ru, rv;
+  float ulo, uhi, vlo, vhi;
+  // The rectangle can be smaller than the macro cell's shadow (detector axes
+  // rotated against the volume axes). Its integer bounds (floor / ceil of the
+  // extremes) decide which samples of the clipped band are taken; the affine
+  // extremes agree with the reference's to ~1e-3 pixel, so they give the
+  // same samples unless the band reaches the nearest sub-pixel sample beyond
+  // an integer bound (0.5 / os). Then the rectangle is evaluated per quad
+  // with the reference's expressions (macro_footprint).
+  int clips;
+};
+
+// Depth of the macro cell's first corner (macro_footprint's corner 0, the
+// reference's expression), which selects the quad's CTF slab.
+__device__ __forceinline__ float macro_depth(const KConst& k, int x, int y, int z) {
+  const float mnx = fadd(k.bbMin.x, fmul((float)x, k.vs.x)), mny = fadd(k.bbMin.y, fmul((float)y, k.vs.y)),
+              mnz = fadd(k.bbMin.z, fmul((float)z, k.vs.z));
+  const float ndet = fadd(fadd(fmul(-k.n.x, k.det.x), -fmul(k.n.y, k.det.y)), -fmul(k.n.z, k.det.z));
+  const float t = fadd(fadd(fmul(k.n.x, mnx), fmul(k.n.y, mny)), fmul(k.n.z, mnz));
+  return fabsf(fadd(t, ndet));
+}
+
+// The reference's macro-cell rectangle (macro_footprint): the cell's 8
+// corners are projected along n onto the detector plane, the bounding box
+// (lo, hi) of those hit points is taken in world coordinates (x swapped when
+// n.x <= 0) and only lo and hi are mapped to the detector. With the hit point
+// h = A p + b linear in the corner p, lo and hi are affine in the quad
+// position, and so are their detector coordinates; the rectangle is the
+// reference's up to float rounding. It can be smaller than the voxels'
+// shadows when the detector axes are rotated against the volume axes, and
+// then clips samples as the reference does.
+__device__ __forceinline__ void macro_rect(const AxisGeom& g, int x, int y, int z, int pw, int ph, int& pbx, int& pby,
+                                           int& pbz, int& pbw) {
+  const float uL = fmaf((float)z, g.ru.z, fmaf((float)y, g.ru.y, fmaf((float)x, g.ru.x, g.ru.w)));
+  const float vL = fmaf((float)z, g.rv.z, fmaf((float)y, g.rv.y, fmaf((float)x, g.rv.x, g.rv.w)));
+  const float plx = uL + g.ulo, phx = uL + g.uhi, ply = vL + g.vlo, phy = vL + g.vhi;
+  pbx = (int)fminf(fmaxf(floorf(fminf(plx, phx)), 0.0f), (float)(pw - 1));
+  pby = (int)fminf(fmaxf(ceilf(fmaxf(plx, phx)), 0.0f), (float)(pw - 1));
+  pbz = (int)fminf(fmaxf(floorf(fminf(ply, phy)), 0.0f), (float)(ph - 1));
+  pbw = (int)fminf(fmaxf(ceilf(fmaxf(ply, phy)), 0.0f), (float)(ph - 1));
+}
+
+inline AxisGeom make_axis_geom(const KConst& k, const BpGeom& b, int os) {
+  AxisGeom g;
+  g.U = b.U;
+  g.V = b.V;
+  g.U0 = b.U0;
+  g.V0 = b.V0;
+  g.hu = b.hu;
+  g.hv = b.hv;
+  // offset d = du * u + dv * v; w = d.x n.z - d.z n.x
+  g.wu = k.u.x * k.n.z - k.u.z * k.n.x;
+  g.wv = k.v.x * k.n.z - k.v.z * k.n.x;
+  g.yu = k.u.y;
+  g.yv = k.v.y;
+  g.hby = b.hb.y;
+  const float anx = fabsf(k.n.x), anz = fabsf(k.n.z);
+  const float hx = b.hb.x, hz = b.hb.z;
+  g.L0 = fminf(anx > 0.f ? 2.f * hx / anx : FLT_MAX, anz > 0.f ? 2.f * hz / anz : FLT_MAX);
+  const float prod = anx * anz;
+  g.K = prod > 1e-30f ? 1.0f / prod : 1e30f;
+  g.w1K = (hx * anz + hz * anx) * g.K;
+  // macro-cell rectangle: h = A p + b with A = I - sg n n^T, b = -sg ndet n,
+  // sg the sign of n.p + ndet over the volume (the detector lies outside it)
+  const double n[3] = {k.n.x, k.n.y, k.n.z};
+  const double det[3] = {k.det.x, k.det.y, k.det.z};
+  const double ndet = -n[0] * det[0] - n[1] * det[1] - n[2] * det[2];
+  const double bmin[3] = {k.bbMin.x, k.bbMin.y, k.bbMin.z}, vs[3] = {k.vs.x, k.vs.y, k.vs.z};
+  const double ext[3] = {5.0 * vs[0], vs[1], vs[2]};  // the 5 x 1 x 1 macro cell
+  const double dim[3] = {k.dim.x, k.dim.y, k.dim.z};
+  double ctr = ndet;  // n.p + ndet at the volume centre
+  for (int j = 0; j < 3; ++j) ctr += n[j] * (bmin[j] + 0.5 * vs[j] * dim[j]);
+  const double sg = ctr < 0.0 ? -1.0 : 1.0;
+  double A[3][3], base[3], dlo[3], dhi[3];
+  for (int r = 0; r < 3; ++r) {
+    base[r] = -sg * ndet * n[r];
+    dlo[r] = dhi[r] = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      A[r][c] = (r == c ? 1.0 : 0.0) - sg * n[r] * n[c];
+      base[r] += A[r][c] * bmin[c];
+      const double e = A[r][c] * ext[c];
+      dlo[r] += e < 0.0 ? e : 0.0;
+      dhi[r] += e > 0.0 ? e : 0.0;
+    }
+  }
+  if (k.n.x <= 0.0f) {  // the reference swaps lo.x and hi.x
+    const double t = dlo[0];
+    dlo[0] = dhi[0];
+    dhi[0] = t;
+  }
+  const double U[3] = {b.U.x, b.U.y, b.U.z}, V[3] = {b.V.x, b.V.y, b.V.z};
+  double ru[4] = {0, 0, 0, b.U0}, rv[4] = {0, 0, 0, b.V0};
+  double ulo = 0, uhi = 0, vlo = 0, vhi = 0;
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) {
+      ru[c] += U[r] * A[r][c] * vs[c];
+      rv[c] += V[r] * A[r][c] * vs[c];
+    }
+    ru[3] += U[r] * base[r];
+    rv[3] += V[r] * base[r];
+    ulo += U[r] * dlo[r];
+    uhi += U[r] * dhi[r];
+    vlo += V[r] * dlo[r];
+    vhi += V[r] * dhi[r];
+  }
+  // true extent of the macro cell's shadow around the projection of A m:
+  // sum_c min/max(0, (U A)_c ext_c); the rectangle clips when its own
+  // extent (U dlo, U dhi) is narrower
+  double su_lo = 0, su_hi = 0, sv_lo = 0, sv_hi = 0;
+  for (int c = 0; c < 3; ++c) {
+    double ua = 0, va = 0;
+    for (int r = 0; r < 3; ++r) {
+      ua += U[r] * A[r][c];
+      va += V[r] * A[r][c];
+    }
+    su_lo += ua * ext[c] < 0 ? ua * ext[c] : 0;
+    su_hi += ua * ext[c] > 0 ? ua * ext[c] : 0;
+    sv_lo += va * ext[c] < 0 ? va * ext[c] : 0;
+    sv_hi += va * ext[c] > 0 ? va * ext[c] : 0;
+  }
+  const double band = fmax(fmax(fmin(ulo, uhi) - su_lo, su_hi - fmax(ulo, uhi)),
+                           fmax(fmin(vlo, vhi) - sv_lo, sv_hi - fmax(vlo, vhi)));
+  g.clips = band > 0.5 / os - 0.01 ? 1 : 0;
+  g.ru = make_float4((float)ru[0], (float)ru[1], (float)ru[2], (float)ru[3]);
+  g.rv = make_float4((float)rv[0], (float)rv[1], (float)rv[2], (float)rv[3]);
+  g.ulo = (float)ulo;
+  g.uhi = (float)uhi;
+  g.vlo = (float)vlo;
+  g.vhi = (float)vhi;
+  return g;
+}
+
+// Whether a projection takes the single-axis sums: beam without a y
+// component, exact sub-pixel lattice, samples read at (px, py).
+inline bool axis_eligible(const KConst& k, const BpGeom& g) {
+  return g.exact_grid && g.aniso_identity && fabsf(k.n.y) <= 1e-6f;
+}
+
+// sum(sample*chord) and sum(chord) of one voxel whose centre projects to
+// (uc, vc), for a single-axis projection. With n.y = 0 the chord of a
+// sample's ray through the voxel depends only on the ray's offset w from the
+// voxel centre perpendicular to n in the x-z plane (a trapezoid: the plateau
+// min(2 hx / |n.x|, 2 hz / |n.z|), falling linearly to 0 at
+// |w| = hx |n.z| + hz |n.x| with slope 1 / (|n.x| |n.z|)), cut to 0 where the
+// offset's y component leaves the voxel. Samples are the sub-pixel grid
+// points (m + 0.5) / os inside the voxel's shadow and inside
+// [mu_min, mu_max] x [mv_min, mv_max] (the quad's macro-cell rectangle);
+// read(mu, mv) returns the image at grid point (mu, mv). SKIP (filtered
+// 4-texel reads): loops with a branch that reads only samples with a
+// nonzero chord; otherwise (one load per sample, pre-sampled images) the
+// first 2 x 3 samples are unrolled and read unconditionally.
+template <bool SKIP, class Read>
+__device__ __forceinline__ void axis_sums(const AxisGeom& g, float uc, float vc, float fos, float inv, float dwv,
+                                          float dyv, int mu_min, int mu_max, int mv_min, int mv_max, const Read& read,
+                                          float& acc, float& dacc) {
+  const int mu0 = max((int)ceilf((uc - g.hu) * fos - 0.5f), mu_min);
+  const int mu1 = min((int)floorf((uc + g.hu) * fos - 0.5f), mu_max);
+  const int mv0 = max((int)ceilf((vc - g.hv) * fos - 0.5f), mv_min);
+  const int mv1 = min((int)floorf((vc + g.hv) * fos - 0.5f), mv_max);
+  const float dv0 = ((float)mv0 + 0.5f) * inv - vc;
+  float a = 0.f, da = 0.f;
+  // a voxel's shadow holds 2-3 sub-pixel samples per axis at OS 2
+  const int rows = mu1 - mu0 + 1;
+  const int cnt = mv1 - mv0 + 1;
+  auto row = [&](int mu) {
+    const float du = ((float)mu + 0.5f) * inv - uc;
+    const float w = du * g.wu + dv0 * g.wv, dy = du * g.yu + dv0 * g.yv;
+    auto body = [&](int j) {
+      const float ww = fmaf((float)j, dwv, w), yy = fmaf((float)j, dyv, dy);
+      float L = fminf(g.L0, fmaxf(0.f, fmaf(-fabsf(ww), g.K, g.w1K)));
+      L = fabsf(yy) <= g.hby ? L : 0.f;
+      if (!SKIP || L > 0.f) {
+        a = fmaf(read(mu, mv0 + j), L, a);
+        da += L;
+      }
+    };
+    if (SKIP) {
+#pragma unroll 1
+      for (int j = 0; j < cnt; ++j) body(j);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        if (j < cnt) body(j);
+#pragma unroll 1
+      for (int j = 3; j < cnt; ++j) body(j);
+    }
+  };
+  if (SKIP) {
+#pragma unroll 1
+    for (int r = 0; r < rows; ++r) row(mu0 + r);
+  } else {
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+      if (r < rows) row(mu0 + r);
+#pragma unroll 1
+    for (int r = 2; r < rows; ++r) row(mu0 + r);
+  }
+  acc = a;
+  dacc = da;
+}
+
+
 }  // namespace bpcore
 }  // namespace esb

@@ -13,8 +13,10 @@
 // quad in registers, adds the tilts in list order and writes the quad once.
 // With CTF, one such launch per tilt reads each quad's slab image from the
 // tilt's slab table. The per-voxel sums are those of the single-volume fast
-// back-projector (esb_bp_core.cuh), added in the same order, so batched and
-// per-particle results agree to float rounding.
+// back-projector (esb_bp_core.cuh: the single-axis sums for projections
+// without a y component of the beam, the general chords otherwise), added in
+// the same order, so batched and per-particle results agree to float
+// rounding.
 #include <string.h>
 
 #include "esb_bp_core.cuh"
@@ -43,10 +45,14 @@ struct SubvolParticle {
 struct PairConst {
   KConst k;
   BpGeom g;
+  AxisGeom a;  // single-axis sums (axis_sums) when axis != 0
+  int axis;
   int active;
 };
 
-__global__ void __launch_bounds__(kQuadsPerItem) k_subvol_batch(const SubvolWork* __restrict__ work, int n_work,
+// AXIS: every pair of the call takes the single-axis sums.
+template <bool AXIS>
+__global__ void __launch_bounds__(kQuadsPerItem, 5) k_subvol_batch(const SubvolWork* __restrict__ work, int n_work,
                                                                 const SubvolParticle* __restrict__ parts,
                                                                 const PairConst* __restrict__ pairs, int n_list,
                                                                 int t0, int nt, const float* __restrict__ imgs,
@@ -80,10 +86,30 @@ __global__ void __launch_bounds__(kQuadsPerItem) k_subvol_batch(const SubvolWork
         img = imgs + (size_t)(t - t0) * img_stride;
       }
       float acc[4], dacc[4];
+      if (AXIS) {
+        const AxisGeom& ag = pc.a;
+        const float cy = pc.k.bbMin.y + ((float)y + 0.5f) * pc.k.vs.y;
+        const float cz = pc.k.bbMin.z + ((float)z + 0.5f) * pc.k.vs.z;
+        const float uyz = ag.U.y * cy + ag.U.z * cz + ag.U0, vyz = ag.V.y * cy + ag.V.z * cz + ag.V0;
+        const bool lin = linear != 0;
+        const bool interior = !lin || (pbx >= 1 && pbz >= 1);
+        auto read = [&](int mu, int mv) -> float {
+          const float px = ((float)mu + 0.5f) * inv, py = ((float)mv + 0.5f) * inv;
+          return interior ? sample_interior(img, (size_t)ph, 1, px, py, lin)
+                          : sample_image(img, pw, ph, (size_t)pw, px, py, lin, true);
+        };
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-        voxel_sums(pc.k, pc.g, img, pw, ph, (size_t)pw, os, inv, linear != 0, true, x + i, y, z, pbx, pby, pbz, pbw,
-                   acc[i], dacc[i]);
+        for (int i = 0; i < 4; ++i) {
+          const float cx = pc.k.bbMin.x + ((float)(x + i) + 0.5f) * pc.k.vs.x;
+          axis_sums<true>(ag, ag.U.x * cx + uyz, ag.V.x * cx + vyz, (float)os, inv, inv * ag.wv, inv * ag.yv,
+                          pbx * os, pby * os - 1, pbz * os, pbw * os - 1, read, acc[i], dacc[i]);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          voxel_sums(pc.k, pc.g, img, pw, ph, (size_t)pw, os, inv, linear != 0, true, x + i, y, z, pbx, pby, pbz,
+                     pbw, acc[i], dacc[i]);
+      }
       // lambda = 1 (weighted back-projection): v += 1 * acc / dacc
       if (dacc[0] > 0.f) v.x += 1.0f * acc[0] / dacc[0];
       if (dacc[1] > 0.f) v.y += 1.0f * acc[1] / dacc[1];
@@ -133,9 +159,15 @@ cudaError_t subvol_batch_build(SubvolBatch& b, int n_particles, float* const* bo
   memcpy(b.host.data(), work.data(), work.size() * sizeof(SubvolWork));
   memcpy(b.host.data() + b.off_parts, parts.data(), parts.size() * sizeof(SubvolParticle));
   PairConst* pc = (PairConst*)(b.host.data() + b.off_pairs);
+  b.all_axis = 1;
   for (size_t i = 0; i < n_pairs; ++i) {
     pc[i].k = consts[i];
     pc[i].g = make_geom(consts[i], os);
+    pc[i].axis = axis_eligible(consts[i], pc[i].g) ? 1 : 0;
+    if (pc[i].axis)
+      pc[i].a = make_axis_geom(consts[i], pc[i].g, os);
+    else
+      b.all_axis = 0;
     pc[i].active = !active || active[i];
   }
   if (bytes > b.cap) {
@@ -159,17 +191,20 @@ cudaError_t subvol_batch_launch(const SubvolBatch& b, int t0, int nt, const floa
   cudaError_t e;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subvol_batch, kQuadsPerItem, 0)) != cudaSuccess)
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+           &per_sm, b.all_axis ? k_subvol_batch<true> : k_subvol_batch<false>, kQuadsPerItem, 0)) != cudaSuccess)
     return e;
   // persistent grid: every resident block slot of every SM, looping over the
   // work list
   long blocks = (long)n_sm * (per_sm > 0 ? per_sm : 1);
   if (blocks > b.n_work) blocks = b.n_work;
   const char* base = (const char*)b.dev;
-  k_subvol_batch<<<(unsigned)blocks, kQuadsPerItem, 0, st>>>(
-      (const SubvolWork*)base, b.n_work, (const SubvolParticle*)(base + b.off_parts),
-      (const PairConst*)(base + b.off_pairs), b.n_list, t0, nt, imgs, img_stride, slabs, pw, ph, os, 1.0f / (float)os,
-      linear); ESB_COUNT_LAUNCH();
+  auto kern = b.all_axis ? k_subvol_batch<true> : k_subvol_batch<false>;
+  kern<<<(unsigned)blocks, kQuadsPerItem, 0, st>>>((const SubvolWork*)base, b.n_work,
+                                                   (const SubvolParticle*)(base + b.off_parts),
+                                                   (const PairConst*)(base + b.off_pairs), b.n_list, t0, nt, imgs,
+                                                   img_stride, slabs, pw, ph, os, 1.0f / (float)os, linear);
+  ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 

@@ -20,6 +20,7 @@ struct SubvolBatch {
   size_t off_parts = 0, off_pairs = 0;
   int n_work = 0;
   int n_list = 0;
+  int all_axis = 0;  // every pair takes the single-axis sums
 };
 
 // True when every box can be updated with aligned float4 accesses (x extent a
