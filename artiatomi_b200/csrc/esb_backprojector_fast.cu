@@ -128,11 +128,15 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
   };
   const long base = ((long)z * ny + y) * (long)k.dim.x + x;
   float res[4], has[4];
+  const bool patch = !UP && os == 2 && lin && interior;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const float cx = k.bbMin.x + ((float)(x + i) + 0.5f) * k.vs.x;
-    axis_sums<!UP>(g, g.U.x * cx + uyz, g.V.x * cx + vyz, fos, inv, dwv, dyv, pbx * os, pby * os - 1, pbz * os,
-                   pbw * os - 1, read, res[i], has[i]);
+    const float uc = g.U.x * cx + uyz, vc = g.V.x * cx + vyz;
+    if (!(patch && axis_sums_os2(g, uc, vc, dwv, dyv, pbx * 2, pby * 2 - 1, pbz * 2, pbw * 2 - 1, img, sx, sy, pw, ph,
+                                 res[i], has[i])))
+      axis_sums<!UP>(g, uc, vc, fos, inv, dwv, dyv, pbx * os, pby * os - 1, pbz * os, pbw * os - 1, read, res[i],
+                     has[i]);
   }
   if (VT == ESB_VOXEL_F32 && (((uintptr_t)((float*)vol + base)) & 15) == 0) {
     float4 v = *((float4*)((float*)vol + base));

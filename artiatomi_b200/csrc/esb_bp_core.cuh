@@ -462,5 +462,74 @@ __device__ __forceinline__ void axis_sums(const AxisGeom& g, float uc, float vc,
 }
 
 
+// axis_sums for oversampling 2 with bilinear reads of an image whose samples
+// all lie in its interior (texel (ix, iy) at img + ix * sx + iy * sy). The
+// sub-pixel samples then sit at quarter-texel offsets: sample m reads the
+// texel pair ((m - 1) >> 1, +1) with weight 0.75 on the second texel for m
+// even and 0.25 for m odd. The (up to) 3 x 3 samples of a voxel's shadow
+// therefore read one 3 x 3 texel patch: it is loaded once, each sample's
+// value is formed from it exactly as sample_interior forms it (x then y),
+// and the samples are weighted by their chords. Returns false (nothing
+// accumulated) when the shadow holds more than 3 samples along an axis.
+__device__ __forceinline__ bool axis_sums_os2(const AxisGeom& g, float uc, float vc, float dwv, float dyv, int mu_min,
+                                              int mu_max, int mv_min, int mv_max, const float* __restrict__ img,
+                                              size_t sx, size_t sy, int pw, int ph, float& acc, float& dacc) {
+  const int mu0 = max((int)ceilf((uc - g.hu) * 2.0f - 0.5f), mu_min);
+  const int mu1 = min((int)floorf((uc + g.hu) * 2.0f - 0.5f), mu_max);
+  const int mv0 = max((int)ceilf((vc - g.hv) * 2.0f - 0.5f), mv_min);
+  const int mv1 = min((int)floorf((vc + g.hv) * 2.0f - 0.5f), mv_max);
+  const int nu = mu1 - mu0 + 1, nv = mv1 - mv0 + 1;
+  if (nu > 3 || nv > 3) return false;
+  if (nu <= 0 || nv <= 0) {
+    acc = 0.f;
+    dacc = 0.f;
+    return true;
+  }
+  const int fxa = (mu0 - 1) >> 1, fya = (mv0 - 1) >> 1;
+  float T[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const size_t col = (size_t)min(fxa + c, pw - 1) * sx;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) T[c][r] = __ldg(img + col + (size_t)min(fya + r, ph - 1) * sy);
+  }
+  const bool ou = (mu0 & 1) != 0, ov = (mv0 & 1) != 0;
+  // sample columns: texel pair and weight of the second texel
+  const float a0 = ou ? 0.25f : 0.75f, a1 = ou ? 0.75f : 0.25f, a2 = a0;
+  const float b0 = ov ? 0.25f : 0.75f, b1 = ov ? 0.75f : 0.25f, b2 = b0;
+  float C[3][3];  // C[i][r]: sample column i interpolated at texel row r
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    C[0][r] = (1.0f - a0) * T[0][r] + a0 * T[1][r];
+    const float l1 = ou ? T[0][r] : T[1][r], h1 = ou ? T[1][r] : T[2][r];
+    C[1][r] = (1.0f - a1) * l1 + a1 * h1;
+    C[2][r] = (1.0f - a2) * T[1][r] + a2 * T[2][r];
+  }
+  const float du0 = ((float)mu0 + 0.5f) * 0.5f - uc, dv0 = ((float)mv0 + 0.5f) * 0.5f - vc;
+  const float w0 = du0 * g.wu + dv0 * g.wv, y0 = du0 * g.yu + dv0 * g.yv;
+  const float dwu = 0.5f * g.wu, dyu = 0.5f * g.yu;
+  float a = 0.f, da = 0.f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float ww = fmaf((float)j, dwv, fmaf((float)i, dwu, w0));
+      const float yy = fmaf((float)j, dyv, fmaf((float)i, dyu, y0));
+      float L = fminf(g.L0, fmaxf(0.f, fmaf(-fabsf(ww), g.K, g.w1K)));
+      L = (fabsf(yy) <= g.hby && i < nu && j < nv) ? L : 0.f;
+      const float bj = j == 0 ? b0 : (j == 1 ? b1 : b2);
+      const float lo = j == 0 ? C[i][0] : (j == 1 ? (ov ? C[i][0] : C[i][1]) : C[i][1]);
+      const float hi = j == 0 ? C[i][1] : (j == 1 ? (ov ? C[i][1] : C[i][2]) : C[i][2]);
+      const float v = (1.0f - bj) * lo + bj * hi;
+      a = fmaf(v, L, a);
+      da += L;
+    }
+  }
+  acc = a;
+  dacc = da;
+  return true;
+}
+
+
 }  // namespace bpcore
 }  // namespace esb

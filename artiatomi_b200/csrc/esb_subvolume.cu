@@ -74,7 +74,12 @@ __global__ void __launch_bounds__(kQuadsPerItem, 5) k_subvol_batch(const SubvolW
       if (!pc.active) continue;
       float depth;
       int pbx, pby, pbz, pbw;
-      macro_footprint(pc.k, x, y, z, pw, ph, depth, pbx, pby, pbz, pbw);
+      if (AXIS && !pc.a.clips) {  // the rectangle from its affine form (macro_rect)
+        depth = macro_depth(pc.k, x, y, z);
+        macro_rect(pc.a, x, y, z, pw, ph, pbx, pby, pbz, pbw);
+      } else {
+        macro_footprint(pc.k, x, y, z, pw, ph, depth, pbx, pby, pbz, pbw);
+      }
       const float* img;
       if (slabs.count > 0) {
         if (!(depth >= slabs.bound[0] && depth < slabs.bound[slabs.count])) continue;
@@ -98,11 +103,15 @@ __global__ void __launch_bounds__(kQuadsPerItem, 5) k_subvol_batch(const SubvolW
           return interior ? sample_interior(img, (size_t)ph, 1, px, py, lin)
                           : sample_image(img, pw, ph, (size_t)pw, px, py, lin, true);
         };
+        const bool patch = os == 2 && lin && interior;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const float cx = pc.k.bbMin.x + ((float)(x + i) + 0.5f) * pc.k.vs.x;
-          axis_sums<true>(ag, ag.U.x * cx + uyz, ag.V.x * cx + vyz, (float)os, inv, inv * ag.wv, inv * ag.yv,
-                          pbx * os, pby * os - 1, pbz * os, pbw * os - 1, read, acc[i], dacc[i]);
+          const float uc = ag.U.x * cx + uyz, vc = ag.V.x * cx + vyz;
+          if (!(patch && axis_sums_os2(ag, uc, vc, inv * ag.wv, inv * ag.yv, pbx * 2, pby * 2 - 1, pbz * 2,
+                                       pbw * 2 - 1, img, (size_t)ph, 1, pw, ph, acc[i], dacc[i])))
+            axis_sums<true>(ag, uc, vc, (float)os, inv, inv * ag.wv, inv * ag.yv, pbx * os, pby * os - 1, pbz * os,
+                            pbw * os - 1, read, acc[i], dacc[i]);
         }
       } else {
 #pragma unroll
