@@ -5,11 +5,13 @@
 // t_j = t_in + j*h', j = 0..J-1, and sums the samples. Within one cell of
 // the interpolation lattice the interpolant is a trilinear polynomial of the
 // cell-local coordinates, and these are linear in j. So the sum over the
-// samples inside a cell has a closed form in the power sums of j. This kernel
-// walks the cells a ray crosses (3-D DDA), loads each cell's 8 corners once
-// (4 when it enters through a face shared with the previous cell) and adds
-// the closed-form sum of that cell's samples. That replaces ~5 trilinear
-// evaluations (40 loads) per cell with 4-8 loads and ~60 FLOPs.
+// samples inside a cell has a closed form in the power sums of j. Rays of a
+// single-axis series stay in one y plane and take the branch-free layer walk
+// (layer_sum_xz: one layer of the major axis per step, two cells per layer);
+// other rays walk the cells they cross with a 3-D DDA (cell_sum), loading
+// each cell's 8 corners once (4 when it enters through a face shared with
+// the previous cell). Either replaces ~5 trilinear evaluations (40 loads)
+// per cell with 4-8 loads and a few dozen FLOPs.
 //
 // The sample positions are the reference's: t is the reference's float
 // recurrence t += 0.15*voxelSize, whose step on the float grid of t ~ 1e4 is
