@@ -187,3 +187,26 @@ def test_fast_kernels_rotated_and_tilted_axes(psi_deg, tilt_x):
                                                                                             projs, il, 2, 2)
         tol = max(tol, 1.5 * rel_l2(ref32, ref))
     assert rel_l2(host(v), ref) <= tol, (rel_l2(host(v), ref), tol)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ctf", [False, True])
+def test_subvolume_wbp_rotated_axis(ctf):
+    """Sub-volume WBP with the tilt axis rotated 37 degrees in the detector
+    plane (single-axis sums, oversampling-2 texel patches, the reference's
+    clipping macro-cell rectangle): batched against per-particle launches,
+    and both against the FP64 oracle within 1.5x the reference's own FP32
+    deviation from it."""
+    from tests.test_parity_fast import _subvolume_case, _subvolume_gpu, _subvolume_oracle
+
+    c = _subvolume_case(ctf, [16, 24, 32, 16], n=7, seed=9, psi_deg=37.0)
+    il = np.arange(c["n"], dtype=np.int32)
+    plain = _subvolume_gpu(c, False, il)
+    batch = _subvolume_gpu(c, True, il)
+    o64 = _subvolume_oracle(c, il)
+    o32 = _subvolume_oracle(c, il, precision=0)
+    for a, b, r64, r32 in zip(plain, batch, o64, o32):
+        assert np.abs(a).sum() > 0
+        assert rel_l2(b, a) <= 1e-5, rel_l2(b, a)
+        tol = max(1e-4 if not ctf else 1e-3, 1.5 * rel_l2(r32, r64))
+        assert rel_l2(b, r64) <= tol, (rel_l2(b, r64), tol)

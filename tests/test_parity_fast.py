@@ -206,13 +206,14 @@ def test_fast_sart_ctf():
         assert e <= tol, (prec, e)
 
 
-def _subvolume_case(ctf, sizes, n=7, seed=31):
+def _subvolume_case(ctf, sizes, n=7, seed=31, psi_deg=0.0):
     import artiatomi_b200 as E
     from artiatomi_b200 import _lib as L
     from oracle import geometry as G
 
     W = H = 96
     tilt = np.linspace(-60, 60, n).astype(np.float32)
+    psi = np.full(n, psi_deg, np.float32)
     rng = np.random.default_rng(seed)
     projs = rng.normal(size=(n, H, W)).astype(np.float32)
     full, fo = E.volume_geometry((96, 96, 40)), G.volume_geometry((96, 96, 40))
@@ -224,14 +225,14 @@ def _subvolume_case(ctf, sizes, n=7, seed=31):
     pair = (L.ProjGeom * (len(sizes) * n))()
     pair_o = []
     for p in range(len(sizes)):
-        g = E.projection_geometry(E.Markers(tilt), W, H, extra_shift=shifts[p])
+        g = E.projection_geometry(E.Markers(tilt, rotation_psi=psi), W, H, extra_shift=shifts[p])
         for i in range(n):
             pair[p * n + i] = g[i]
-        pair_o.append(G.projection_geometry(tilt, width=W, height=H, extra_shift=shifts[p]))
+        pair_o.append(G.projection_geometry(tilt, psi=psi, width=W, height=H, extra_shift=shifts[p]))
     defocus = np.stack([np.full(n, 3000.0), np.full(n, 3100.0), np.full(n, 20.0)], 1).astype(np.float32).ravel()
     cfgd = dict(oversampling=2, ctf_mode=ctf, pixel_size_nm=0.27, ctf_slice_thickness_nm=4.0,
                 ctf_beta_fac=(10.0, 0.0, 0.008, 0.0))
-    return dict(W=W, H=H, n=n, tilt=tilt, projs=projs, full=full, fo=fo, sub=sub, subo=subo, pair=pair,
+    return dict(W=W, H=H, n=n, tilt=tilt, psi=psi, projs=projs, full=full, fo=fo, sub=sub, subo=subo, pair=pair,
                 pair_o=pair_o, defocus=defocus if ctf else None, cfgd=cfgd, shifts=shifts, sizes=sizes)
 
 
@@ -239,7 +240,7 @@ def _subvolume_gpu(c, batched, index_list, active=None):
     import artiatomi_b200 as E
 
     W, H, n = c["W"], c["H"], c["n"]
-    pg = E.projection_geometry(E.Markers(c["tilt"]), W, H)
+    pg = E.projection_geometry(E.Markers(c["tilt"], rotation_psi=c["psi"]), W, H)
     rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **c["cfgd"]), pg, c["tilt"], c["defocus"])
     boxes = [cuda(np.zeros((s, s, s), np.float32)) for s in c["sizes"]]
     rec.subvolume_wbp(c["full"], c["sub"], c["pair"], boxes, cuda(c["projs"]), index_list, active=active,
@@ -247,13 +248,13 @@ def _subvolume_gpu(c, batched, index_list, active=None):
     return [host(b) for b in boxes]
 
 
-def _subvolume_oracle(c, index_list, active=None):
+def _subvolume_oracle(c, index_list, active=None, precision=1):
     from oracle import geometry as G
     from oracle.driver import OracleReconstructor
 
     W, H = c["W"], c["H"]
-    orc = OracleReconstructor(c["cfgd"], W, H, G.projection_geometry(c["tilt"], width=W, height=H), c["tilt"],
-                              c["defocus"], precision=1)
+    orc = OracleReconstructor(c["cfgd"], W, H, G.projection_geometry(c["tilt"], psi=c["psi"], width=W, height=H),
+                              c["tilt"], c["defocus"], precision=precision)
     bo = [np.zeros((s, s, s), np.float32) for s in c["sizes"]]
     orc.subvolume_wbp(c["fo"], c["subo"], c["pair_o"], bo, c["projs"], index_list, active=active)
     return bo
