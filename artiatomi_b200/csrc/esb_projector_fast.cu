@@ -287,15 +287,17 @@ __device__ float ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0,
 
 // mode 0: march (proj += sum/4, dist = mean chord); mode 1: slicer (proj += sum/4 within [tmin, tmax])
 template <int VT, int MODE>
-__global__ void __launch_bounds__(256, 3) k_project_fast(KConst c, const void* __restrict__ vol, float* __restrict__ proj,
+__global__ void __launch_bounds__(128, 6) k_project_fast(KConst c, const void* __restrict__ vol, float* __restrict__ proj,
                                                       float* __restrict__ dist, size_t pitchE, float tminDef,
                                                       float tmaxDef, int x0, int y0, int x1, int y1) {
-  // lanes: 4 sub-rays of a pixel adjacent; a warp spans 8 detector rows (v)
+  // lanes: 4 sub-rays of a pixel adjacent; a warp spans 8 detector rows (v);
+  // 4 warps per block: 4 detector columns (u). Blocks of 128 threads fit 6
+  // per SM at the walker's register count, where 256-thread blocks fit 3.
   const int lane = threadIdx.x & 31;
   const int sub = lane & 3;
   const int row = (threadIdx.x >> 2) & 7;
-  const int warp = threadIdx.x >> 5;  // 8 warps per block: 8 detector columns (u)
-  const int x = x0 + (int)blockIdx.x * 8 + warp;
+  const int warp = threadIdx.x >> 5;
+  const int x = x0 + (int)blockIdx.x * 4 + warp;
   const int y = y0 + (int)blockIdx.y * 8 + row;
   const bool active = x < x1 && y < y1;
   Cell<VT> C{vol, (int)c.dim.x, (int)c.dim.y, (int)c.dim.z, (long)c.dim.x, (long)c.dim.x * (long)c.dim.y};
@@ -333,14 +335,14 @@ __global__ void __launch_bounds__(256, 3) k_project_fast(KConst c, const void* _
 // walk the union of their slab ranges together so each slab's sum keeps the
 // reference's sub-ray order.
 template <int VT>
-__global__ void __launch_bounds__(256, 3) k_slicer_fused(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
+__global__ void __launch_bounds__(128, 6) k_slicer_fused(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
                                                       size_t img_stride, size_t pitchE, SlabTable slabs, int x0, int y0,
                                                       int x1, int y1) {
   const int lane = threadIdx.x & 31;
   const int sub = lane & 3;
   const int row = (threadIdx.x >> 2) & 7;
   const int warp = threadIdx.x >> 5;
-  const int x = x0 + (int)blockIdx.x * 8 + warp;
+  const int x = x0 + (int)blockIdx.x * 4 + warp;
   const int y = y0 + (int)blockIdx.y * 8 + row;
   const bool active = x < x1 && y < y1;
   Cell<VT> C{vol, (int)c.dim.x, (int)c.dim.y, (int)c.dim.z, (long)c.dim.x, (long)c.dim.x * (long)c.dim.y};
@@ -393,7 +395,7 @@ cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float*
                                 cudaStream_t st) {
   if (x1 <= x0 || y1 <= y0 || slabs.count <= 0) return cudaSuccess;
   if ((double)c.dim.x * c.dim.y * c.dim.z > 4294967295.0) return cudaErrorInvalidValue;  // 32-bit voxel offsets
-  dim3 blk(256), grd((x1 - x0 + 7) / 8, (y1 - y0 + 7) / 8);
+  dim3 blk(128), grd((x1 - x0 + 3) / 4, (y1 - y0 + 7) / 8);
   if (vt == ESB_VOXEL_F32)
     k_slicer_fused<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
   else if (vt == ESB_VOXEL_F16)
@@ -409,7 +411,7 @@ cudaError_t launch_project_fast(const KConst& c, const void* vol, int vt, int mo
                                 cudaStream_t st) {
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
   if ((double)c.dim.x * c.dim.y * c.dim.z > 4294967295.0) return cudaErrorInvalidValue;  // 32-bit voxel offsets
-  dim3 blk(256), grd((x1 - x0 + 7) / 8, (y1 - y0 + 7) / 8);
+  dim3 blk(128), grd((x1 - x0 + 3) / 4, (y1 - y0 + 7) / 8);
 #define ESB_LAUNCH(VT, M)                                                                            \
   do {                                                                                               \
     k_project_fast<VT, M><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, tmin, tmax, x0, y0, x1, y1); \
