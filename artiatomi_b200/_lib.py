@@ -96,6 +96,9 @@ _SIGS = {
     "esb_bp_fast": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, I, F, F, I, P], I),
     "esb_fp_adjoint": ([C.POINTER(Constants), P, I, I, P, SZ, F, F, P], I),
     "esb_projection_loss_grad": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, F, P, P, P, P], I),
+    "esb_projection_loss_grad_roi": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, F, P, P, P, P, P], I),
+    "esb_rotation_matrix": ([F, F, F, P], I),
+    "esb_rotate_volume": ([P, P, I, P, P], I),
     "esb_make_square": ([I, I, SZ, P, I, P, I, I, I, I, P], I),
     "esb_ctf": ([P, I, F, F, F, I, I, F, P, F, F, F, F, P], I),
     "esb_wbp_weighting": ([P, I, F, I, P], I),

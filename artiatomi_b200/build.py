@@ -33,6 +33,7 @@ UNITS = [
     ("esb_backprojector_fast.cu", []),
     ("esb_subvolume.cu", []),
     ("esb_adjoint.cu", []),
+    ("esb_refine.cu", []),
     ("esb_image.cu", ["--fmad=false"]),
     ("esb_api.cu", []),
     ("esb_noalloc.cu", []),

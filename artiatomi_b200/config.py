@@ -108,9 +108,18 @@ class EmSartConfig:
     NamingConvention: int = 0  # NC_ParticleOnly, 1 NC_TomogramParticle
     ScaleMotivelistShift: float = 1.0
     ScaleMotivelistPosition: float = 1.0
+    # EmSartRefine (REFINE_MODE keys of utils/Config.cpp:408-470)
+    Reference: str = ""
+    ShiftOutputFile: str = ""
+    GroupMode: str = "ByGroup"
+    GroupSize: int = 0
+    MaxDistance: float = 0.0
+    SpeedUpDistance: int = 0
+    MultiPeakDetection: bool = False
+    CCMapFileName: str = ""
 
     @classmethod
-    def from_text(cls, text: str, subvolumes: bool = False) -> "EmSartConfig":
+    def from_text(cls, text: str, subvolumes: bool = False, refine: bool = False) -> "EmSartConfig":
         s = parse_config(text)
         c = cls()
 
@@ -197,11 +206,30 @@ class EmSartConfig:
             c.NamingConvention = 1 if opt("NamingConvention", "") in ("TomoParticle", "Tomo_Particle") else 0
             c.ScaleMotivelistShift = float(req("ScaleMotivelistShift"))
             c.ScaleMotivelistPosition = float(req("ScaleMotivelistPosition"))
+        if refine:
+            c.SizeSubVol = int(float(req("SizeSubVol")))
+            c.VoxelSizeSubVol = float(req("VoxelSizeSubVol"))
+            c.MotiveList = req("MotiveList")
+            c.Reference = req("Reference")
+            c.MaxShift = int(float(req("MaxShift")))
+            c.ShiftOutputFile = req("ShiftOutputFile")
+            c.GroupMode = req("GroupMode")
+            if c.GroupMode not in ("ByGroup", "MaxDistance", "MaxCount"):
+                raise ValueError("GroupMode: ByGroup, MaxDistance or MaxCount expected")
+            if c.GroupMode == "MaxDistance":
+                c.MaxDistance = float(req("MaxDistance"))
+            if c.GroupMode == "MaxCount":
+                c.GroupSize = int(float(req("GroupSize")))
+            c.CCMapFileName = opt("CCMapFileName", "")
+            c.SpeedUpDistance = int(float(req("SpeedUpDistance")))
+            c.ScaleMotivelistShift = float(req("ScaleMotivelistShift"))
+            c.ScaleMotivelistPosition = float(req("ScaleMotivelistPosition"))
+            c.MultiPeakDetection = _bool(req("MultiPeakDetection"))
         return c
 
     @classmethod
-    def from_file(cls, path: str, subvolumes: bool = False) -> "EmSartConfig":
+    def from_file(cls, path: str, subvolumes: bool = False, refine: bool = False) -> "EmSartConfig":
         with open(path) as f:
-            return cls.from_text(f.read(), subvolumes)
+            return cls.from_text(f.read(), subvolumes, refine)
 
 

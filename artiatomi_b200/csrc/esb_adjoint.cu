@@ -325,8 +325,9 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // out: [0] loss, [1] dL/ds_u, [2] dL/ds_v, [3..5] Gauss-Newton terms
-// sum (dp/ds_u)^2, sum dp/ds_u dp/ds_v, sum (dp/ds_v)^2 (all added to).
-template <int VT>
+// sum (dp/ds_u)^2, sum dp/ds_u dp/ds_v, sum (dp/ds_v)^2, and with NOUT = 8
+// [6] sum p^2, [7] sum p * b (all added to).
+template <int VT, int NOUT>
 __global__ void __launch_bounds__(256) k_loss_grad(KConst c, const void* __restrict__ vol,
                                                    const float* __restrict__ meas, size_t pitchE, float sx, float sy,
                                                    float* __restrict__ grad, float* __restrict__ proj_out,
@@ -353,13 +354,16 @@ __global__ void __launch_bounds__(256) k_loss_grad(KConst c, const void* __restr
     }
   }
   const float sum4 = quad_sum_ordered(sum), gx4 = quad_sum_ordered(gx), gy4 = quad_sum_ordered(gy);
-  double part[6] = {0, 0, 0, 0, 0, 0};
+  double part[NOUT];
+#pragma unroll
+  for (int q = 0; q < NOUT; ++q) part[q] = 0.0;
   float r = 0.f;
   if (P.active && P.sub == 0) {
     const size_t i = (size_t)P.y * pitchE + P.x;
     const float p = sum4 * kappa;
     if (proj_out) proj_out[i] = p;
-    r = meas ? p - meas[i] : p;
+    const float b = meas ? meas[i] : 0.f;
+    r = p - b;
     const double dr = r, du = (double)gx4 * kappa, dv = (double)gy4 * kappa;
     part[0] = 0.5 * dr * dr;
     part[1] = dr * du;
@@ -367,17 +371,21 @@ __global__ void __launch_bounds__(256) k_loss_grad(KConst c, const void* __restr
     part[3] = du * du;
     part[4] = du * dv;
     part[5] = dv * dv;
+    if (NOUT == 8) {
+      part[NOUT - 2] = (double)p * p;
+      part[NOUT - 1] = (double)p * b;
+    }
   }
-  // block reduction of the six partial sums, then one FP64 atomic each
-  __shared__ double red[8][6];
+  // block reduction of the partial sums, then one FP64 atomic each
+  __shared__ double red[8][NOUT];
   const int warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
+  for (int q = 0; q < NOUT; ++q) {
     const double v = warp_sum(part[q]);
     if (P.lane == 0) red[warp][q] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 6) {
+  if (threadIdx.x < NOUT) {
     double v = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
     atomicAdd(out + threadIdx.x, v);
@@ -401,20 +409,26 @@ cudaError_t launch_fp_adjoint(const KConst& c, float* grad, const float* img, si
 }
 
 cudaError_t launch_loss_grad(const KConst& c, const void* vol, int vt, const float* meas, size_t pitchE, float sx,
-                             float sy, float* grad, float* proj_out, double* out, int w, int h, cudaStream_t st) {
+                             float sy, float* grad, float* proj_out, double* out, int w, int h, cudaStream_t st,
+                             const int* roi) {
   if (w <= 0 || h <= 0) return cudaSuccess;
-  dim3 blk(256), grd((w + 7) / 8, (h + 7) / 8);
-  switch (vt) {
-    case ESB_VOXEL_F32:
-      k_loss_grad<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, meas, pitchE, sx, sy, grad, proj_out, out, 0, 0, w, h);
-      break;
-    case ESB_VOXEL_F16:
-      k_loss_grad<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, meas, pitchE, sx, sy, grad, proj_out, out, 0, 0, w, h);
-      break;
-    default:
-      k_loss_grad<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, meas, pitchE, sx, sy, grad, proj_out, out, 0, 0, w, h);
-      break;
+  // pixels [x0, x1) x [y0, y1): the whole detector, or a region of it (then
+  // 8 sums, with the amplitude moments)
+  const int x0 = roi ? roi[0] : 0, y0 = roi ? roi[1] : 0, x1 = roi ? roi[2] : w, y1 = roi ? roi[3] : h;
+  if (x1 <= x0 || y1 <= y0) return cudaSuccess;
+  dim3 blk(256), grd((x1 - x0 + 7) / 8, (y1 - y0 + 7) / 8);
+#define ESB_LG(VT, N) \
+  k_loss_grad<VT, N><<<grd, blk, 0, st>>>(c, vol, meas, pitchE, sx, sy, grad, proj_out, out, x0, y0, x1, y1)
+  if (roi) {
+    if (vt == ESB_VOXEL_F32) ESB_LG(ESB_VOXEL_F32, 8);
+    else if (vt == ESB_VOXEL_F16) ESB_LG(ESB_VOXEL_F16, 8);
+    else ESB_LG(ESB_VOXEL_BF16, 8);
+  } else {
+    if (vt == ESB_VOXEL_F32) ESB_LG(ESB_VOXEL_F32, 6);
+    else if (vt == ESB_VOXEL_F16) ESB_LG(ESB_VOXEL_F16, 6);
+    else ESB_LG(ESB_VOXEL_BF16, 6);
   }
+#undef ESB_LG
   ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }

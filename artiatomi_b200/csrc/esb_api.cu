@@ -58,7 +58,9 @@ cudaError_t launch_ctf_slabs(const float* in, float* out, size_t out_stride, int
 cudaError_t launch_fp_adjoint(const KConst& c, float* grad, const float* img, size_t pitchE, float sx, float sy, int w,
                               int h, cudaStream_t st);
 cudaError_t launch_loss_grad(const KConst& c, const void* vol, int vt, const float* meas, size_t pitchE, float sx,
-                             float sy, float* grad, float* proj_out, double* out, int w, int h, cudaStream_t st);
+                             float sy, float* grad, float* proj_out, double* out, int w, int h, cudaStream_t st,
+                             const int* roi = nullptr);
+cudaError_t launch_rotate_volume(const float* in, float* out, int size, const float rot[9], cudaStream_t st);
 cudaError_t launch_convert_input(const void* in, int type, long n, float* out, cudaStream_t st);
 cudaError_t launch_window_stats(const float* img, size_t pitchE, int x0, int y0, int w, int h, double* out,
                                 cudaStream_t st);
@@ -286,6 +288,31 @@ int esb_projection_loss_grad(const esb_constants* c, const void* vol, int voxel_
     return fail(ESB_ERR_INVALID_ARGUMENT, "esb_projection_loss_grad: invalid argument");
   ESB_CK(launch_loss_grad(to_kconst(*c), vol, voxel_type, measured, pitch / 4, shift_u, shift_v, grad_vol, proj_out,
                           out6, proj_x, proj_y, as_stream(stream)), "esb_projection_loss_grad");
+  return ok();
+}
+
+int esb_projection_loss_grad_roi(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y,
+                                 const float* measured, size_t pitch, float shift_u, float shift_v, const int roi[4],
+                                 float* grad_vol, float* proj_out, double* out8, void* stream) {
+  int r;
+  if ((r = check_constants(c, "esb_projection_loss_grad_roi")) ||
+      (r = check_image(proj_x, proj_y, pitch, "esb_projection_loss_grad_roi")))
+    return r;
+  if (!vol || !out8 || !roi || !valid_vt(voxel_type))
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_projection_loss_grad_roi: invalid argument");
+  const int box[4] = {std::max(roi[0], 0), std::max(roi[1], 0), std::min(roi[2], proj_x), std::min(roi[3], proj_y)};
+  ESB_CK(launch_loss_grad(to_kconst(*c), vol, voxel_type, measured, pitch / 4, shift_u, shift_v, grad_vol, proj_out,
+                          out8, proj_x, proj_y, as_stream(stream), box), "esb_projection_loss_grad_roi");
+  return ok();
+}
+
+int esb_rotate_volume(const float* in, float* out, int size, const float rot[9], void* stream) {
+  if (!in || !out || !rot || size <= 0 || size > 2048)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rotate_volume: invalid argument");
+  const size_t bytes = (size_t)size * size * size * sizeof(float);
+  if ((const char*)in < (const char*)out + bytes && (const char*)out < (const char*)in + bytes)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rotate_volume: in and out overlap");
+  ESB_CK(launch_rotate_volume(in, out, size, rot, as_stream(stream)), "esb_rotate_volume");
   return ok();
 }
 

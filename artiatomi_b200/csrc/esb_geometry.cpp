@@ -288,6 +288,46 @@ int esb_mag_aniso_matrix(float amount, float angle_deg, float dim_x, float dim_y
   return esb::ok();
 }
 
+int esb_rotation_matrix(float phi, float psi, float theta, float out[9]) {
+  if (!out) return esb::fail(ESB_ERR_INVALID_ARGUMENT, "esb_rotation_matrix: out is NULL");
+  // RotKernel::computeRotMat (Kernels.cpp:1227-1327): ZXZ Euler angles in
+  // degrees; multiples of 30 and 45 degrees in [0, 330] take exact cosines
+  // and sines (the square roots in float), other angles cosf / sinf of the
+  // angle in radians.
+  const float r3 = sqrtf(3.0f) / 2.0f, r2 = sqrtf(2.0f) / 2.0f;
+  static const float deg[16] = {0, 30, 45, 60, 90, 120, 135, 150, 180, 210, 225, 240, 270, 300, 315, 330};
+  const float cs[16] = {1.0f, r3, r2, 0.5f, 0.0f, -0.5f, -r2, -r3, -1.0f, -r3, -r2, -0.5f, 0.0f, 0.5f, r2, r3};
+  const float sn[16] = {0.0f, 0.5f, r2, r3, 1.0f, r3, r2, 0.5f, 0.0f, -0.5f, -r2, -r3, -1.0f, -r3, -r2, -0.5f};
+  auto cos_sin = [&](float a, float& c, float& s) {
+    for (int i = 0; i < 16; ++i)
+      if (deg[i] == a) {
+        c = cs[i];
+        s = sn[i];
+        return;
+      }
+    const float r = a * (float)M_PI / 180.0f;
+    c = cosf(r);
+    s = sinf(r);
+  };
+  float cphi, sphi, cpsi, spsi, cth, sth;
+  cos_sin(phi, cphi, sphi);
+  cos_sin(psi, cpsi, spsi);
+  cos_sin(theta, cth, sth);
+  float R[3][3];
+  R[0][0] = cpsi * cphi - cth * spsi * sphi;
+  R[1][0] = spsi * cphi + cth * cpsi * sphi;
+  R[2][0] = sth * sphi;
+  R[0][1] = -cpsi * sphi - cth * spsi * cphi;
+  R[1][1] = -spsi * sphi + cth * cpsi * cphi;
+  R[2][1] = sth * cphi;
+  R[0][2] = sth * spsi;
+  R[1][2] = -sth * cpsi;
+  R[2][2] = cth;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) out[3 * r + c] = R[r][c];
+  return esb::ok();
+}
+
 int esb_set_constant_values(const esb_proj_geom* p, const esb_vol_geom* v, const float mag_aniso[9],
                             const float mag_aniso_inv[9], int for_bp, esb_constants* out) {
   if (!p || !v || !out) return esb::fail(ESB_ERR_INVALID_ARGUMENT, "esb_set_constant_values: NULL argument");

@@ -122,6 +122,24 @@ def mag_aniso_matrix(amount: float, angle_deg: float, dim_x: float, dim_y: float
     return out
 
 
+def rotation_matrix(phi: float, psi: float, theta: float) -> np.ndarray:
+    """RotKernel::computeRotMat: 3 x 3 rotation of the motive list's Euler
+    angles (degrees, ZXZ)."""
+    out = np.zeros(9, np.float32)
+    check(lib.esb_rotation_matrix(float(phi), float(psi), float(theta), fptr(out)))
+    return out.reshape(3, 3)
+
+
+def rotate_volume(vol, out, rot, stream=None) -> None:
+    """`rot3d`: out = vol (size^3 FP32, device) rotated about voxel size // 2
+    by rot (rotation_matrix), trilinear with clamp addressing."""
+    size = int(vol.shape[0])
+    if tuple(vol.shape) != (size, size, size) or tuple(out.shape) != (size, size, size):
+        raise ValueError("rotate_volume: cubic volumes of equal size expected")
+    r = np.ascontiguousarray(np.asarray(rot, np.float32).reshape(9))
+    check(lib.esb_rotate_volume(fptr(vol), fptr(out), size, fptr(r), _stream(stream)))
+
+
 IDENTITY3 = np.eye(3, dtype=np.float32).ravel()
 
 
@@ -213,6 +231,18 @@ def fp_adjoint(c: L.Constants, grad, img, shift=(0.0, 0.0), stream=None) -> None
     w, h, pitch = _img_args(img)
     check(lib.esb_fp_adjoint(C.byref(c), fptr(grad), w, h, fptr(img), pitch, float(shift[0]), float(shift[1]),
                              _stream(stream)))
+
+
+def projection_loss_grad_roi(c: L.Constants, vol, measured, out, roi, shift=(0.0, 0.0), grad=None, proj_out=None,
+                             stream=None) -> None:
+    """projection_loss_grad over the detector pixels roi = (x0, y0, x1, y1)
+    (end exclusive) only; `out` holds 8 float64: the 6 sums of
+    projection_loss_grad, then sum p^2 and sum p * measured."""
+    w, h, pitch = _img_args(measured)
+    box = np.ascontiguousarray(np.asarray(roi, np.int32).reshape(4))
+    check(lib.esb_projection_loss_grad_roi(C.byref(c), fptr(vol), _voxel_type_of(vol), w, h, fptr(measured), pitch,
+                                           float(shift[0]), float(shift[1]), fptr(box), fptr(grad),
+                                           fptr(proj_out), fptr(out), _stream(stream)))
 
 
 def projection_loss_grad(c: L.Constants, vol, measured, out, shift=(0.0, 0.0), grad=None, proj_out=None,

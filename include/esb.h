@@ -129,6 +129,11 @@ int esb_subvolume_geometry(int size, float vs_sub, const esb_vol_geom* vol, cons
 /* Reconstructor::GetMagAnistropyMatrix (Reconstructor.cpp:386-426). */
 int esb_mag_aniso_matrix(float amount, float angle_deg, float dim_x, float dim_y, float out[9]);
 
+/* RotKernel::computeRotMat (Kernels.cpp:1227-1327): rotation matrix of the
+ * motive list's Euler angles phi, psi, theta (degrees, ZXZ), row-major;
+ * multiples of 30 and 45 degrees take exact cosines and sines. */
+int esb_rotation_matrix(float phi, float psi, float theta, float out[9]);
+
 /* SetConstantValues (Kernels.cpp:949-1101): assembles the kernel constants
  * of projection `p` and sub-volume `v`. for_bp selects the BP variant, which
  * sets c_zShiftForPartialVolume to the sub-volume's z shift; the FP variant
@@ -235,6 +240,22 @@ int esb_fp_adjoint(const esb_constants* c, float* grad_vol, int proj_x, int proj
 int esb_projection_loss_grad(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y,
                              const float* measured, size_t pitch, float shift_u, float shift_v, float* grad_vol,
                              float* proj_out, double* out6, void* stream);
+
+/* esb_projection_loss_grad over the detector pixels [roi[0], roi[2]) x
+ * [roi[1], roi[3]) only (a particle's footprint), with two more sums for a
+ * fitted amplitude: out8[6] += sum p^2 and out8[7] += sum p * measured
+ * (p = A(x, s)); out8[0..5] as out6. */
+int esb_projection_loss_grad_roi(const esb_constants* c, const void* vol, int voxel_type, int proj_x, int proj_y,
+                                 const float* measured, size_t pitch, float shift_u, float shift_v, const int roi[4],
+                                 float* grad_vol, float* proj_out, double* out8, void* stream);
+
+/* RotKernel::operator() -> `rot3d` (Kernels.cpp:1338-1381,
+ * wbpWeighting.cu:389-405): out = in rotated about voxel (size/2, size/2,
+ * size/2) (integer division): out(p) = in at c + R^T (p - c), trilinear with
+ * clamp addressing, R = rot (esb_rotation_matrix). in, out: size^3 FP32
+ * device buffers, [z][y][x], not overlapping. The reference samples through
+ * a texture (8-bit filter weights); the weights here are FP32. */
+int esb_rotate_volume(const float* in, float* out, int size, const float rot[9], void* stream);
 
 /* CopyToSquareKernel::operator() (Kernels.cpp:808-850) -> `makeSquare`
  * (CopyToSquare.cu:38-92); out is dense maxsize x maxsize. */

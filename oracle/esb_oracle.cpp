@@ -557,6 +557,26 @@ void c2r_2d(const std::complex<float>* in, float* out, int n, int nthreads) {
 // =====================================================================
 extern "C" {
 
+// Kernel `rot3d` (wbpWeighting.cu:389-405) as RotKernel::operator()
+// launches it (Kernels.cpp:1338-1381): output voxel p = size^3 input read
+// through tex3D at c + R^T (p - c) + 0.5, c = size / 2 (integer division),
+// rot row-major [3][3]. q9: 8-bit filter weights.
+int orc_rotate_volume(const float* in, float* out, int size, const float* rot, int q9, int nthreads) {
+  VolView vv{in, size, size, size, 0};
+  const float c = (float)(size / 2);
+  parallel_for(size * size, nthreads, [&](int zy) {
+    const int z = zy / size, y = zy % size;
+    for (int x = 0; x < size; ++x) {
+      const float vx = (float)x - c, vy = (float)y - c, vz = (float)z - c;
+      const float px = c + rot[0] * vx + rot[3] * vy + rot[6] * vz;
+      const float py = c + rot[1] * vx + rot[4] * vy + rot[7] * vz;
+      const float pz = c + rot[2] * vx + rot[5] * vy + rot[8] * vz;
+      out[((size_t)z * size + y) * size + x] = tex3d<float>(vv, px + 0.5f, py + 0.5f, pz + 0.5f, q9 != 0);
+    }
+  });
+  return 0;
+}
+
 // Kernel `march` over the ROI (ForwardProjectionRayMarcher_TL.cu:58-160).
 // precision: 0 = FP32, 1 = FP64.  proj/dist are dense [proj_y][proj_x].
 int orc_fp_march(const OrcGeom* g, const void* vol, int dtype, int proj_x, int proj_y, float* proj, float* dist,

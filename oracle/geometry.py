@@ -258,6 +258,39 @@ def mag_aniso(amount, angle_deg, dimx, dimy):
     return acc.ravel()
 
 
+def rotation_matrix(phi, psi, theta):
+    """RotKernel::computeRotMat (Kernels.cpp:1227-1327), float: multiples of
+    30 and 45 degrees in [0, 330] take exact table values, other angles the
+    float cosine / sine of the angle in radians. Row-major [3][3]."""
+    r3, r2 = f(f(np.sqrt(f(3))) / f(2)), f(f(np.sqrt(f(2))) / f(2))
+    table = {0: (1, 0), 30: (r3, 0.5), 45: (r2, r2), 60: (0.5, r3), 90: (0, 1), 120: (-0.5, r3), 135: (-r2, r2),
+             150: (-r3, 0.5), 180: (-1, 0), 210: (-r3, -0.5), 225: (-r2, -r2), 240: (-0.5, -r3), 270: (0, -1),
+             300: (0.5, -r3), 315: (r2, -r2), 330: (r3, -0.5)}
+
+    def cs(a):
+        a = f(a)
+        for d, (c, s) in table.items():
+            if a == f(d):
+                return f(c), f(s)
+        r = f(f(a * f(math.pi)) / f(180))
+        return f(np.cos(r)), f(np.sin(r))
+
+    cphi, sphi = cs(phi)
+    cpsi, spsi = cs(psi)
+    cth, sth = cs(theta)
+    R = np.zeros((3, 3), np.float32)
+    R[0, 0] = f(f(cpsi * cphi) - f(f(cth * spsi) * sphi))
+    R[1, 0] = f(f(spsi * cphi) + f(f(cth * cpsi) * sphi))
+    R[2, 0] = f(sth * sphi)
+    R[0, 1] = f(f(-cpsi * sphi) - f(f(cth * spsi) * cphi))
+    R[1, 1] = f(f(-spsi * sphi) + f(f(cth * cpsi) * cphi))
+    R[2, 1] = f(sth * cphi)
+    R[0, 2] = f(sth * spsi)
+    R[1, 2] = f(-sth * cpsi)
+    R[2, 2] = cth
+    return R
+
+
 def index_list_random_start_zero(tilt, good=None):
     """Projection::CreateProjectionIndexList(PLT_RANDOM_START_ZERO_TILT)
     (Projection.cpp:592-624) with the C library's srand(0)/rand()."""

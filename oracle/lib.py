@@ -20,6 +20,7 @@ class OrcGeom(C.Structure):
 
 _SIGS = {
     "orc_fp_march": [C.POINTER(OrcGeom), P, I, I, I, P, P, I, I, I, I, I, I, I, I],
+    "orc_rotate_volume": [P, P, I, P, I, I],
     "orc_fp_slicer": [C.POINTER(OrcGeom), P, I, I, I, P, F, F, I, I, I, I],
     "orc_vol_traversal_length": [C.POINTER(OrcGeom), I, I, P, I, I],
     "orc_compare": [I, I, P, P, P, F, P, P, F],

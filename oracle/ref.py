@@ -29,6 +29,7 @@ _SIGS = {
     "ref_wbp_weighting": [P, I, F, I],
     "ref_fourier_filter": [P, I, F, F, F, F],
     "ref_dose_weighting": [P, I, F, F],
+    "ref_rot3d": [P, P, I, P, I, I],
 }
 
 _lib = None

@@ -31,3 +31,23 @@ extern "C" int ref_dose_weighting(float* spec, int n, float dose, float pixelsiz
   });
   return 0;
 }
+
+// Kernel `rot3d` as RotKernel::operator() launches it (Kernels.cpp:1338-1381):
+// 8^3 blocks over the size^3 output, the input bound to `texVol` (linear
+// filtering, clamp addressing). The kernel has no bounds check: size must be
+// a multiple of 8.
+extern "C" int ref_rot3d(const float* in, float* out, int size, const float* rot, int weight8, int nthreads) {
+  if (size <= 0 || size % 8) return 1;
+  EsbSoftTexture t;
+  t.data = in;
+  t.dims = 3;
+  t.nx = t.ny = t.nz = size;
+  t.linear = 1;
+  t.weight8 = weight8;
+  ref_wbp::texVol.bound = &t;
+  const float3 r0 = make_float3(rot[0], rot[1], rot[2]), r1 = make_float3(rot[3], rot[4], rot[5]),
+               r2 = make_float3(rot[6], rot[7], rot[8]);
+  esb_grid(dim3(size / 8, size / 8, size / 8), dim3(8, 8, 8), nthreads,
+           [&]() { ref_wbp::rot3d(size, r0, r1, r2, out); });
+  return 0;
+}

@@ -1,0 +1,268 @@
+"""EmSartRefine's pieces: the rotation of the particle reference (RotKernel /
+rot3d), the region-restricted projection loss with amplitude moments, the
+refine-mode configuration, and the shift refinement end to end
+(artiatomi_b200.refine) on a synthetic tilt series with known extra shifts.
+
+The oracle's rotation is pinned to the reference's own rot3d kernel compiled
+for the host (oracle/_ref); the CUDA rotation is checked against the oracle.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import cuda, host, rel_l2
+
+ANGLES = [(0.0, 0.0, 0.0), (30.0, 45.0, 90.0), (10.5, -20.25, 33.3), (330.0, 135.0, 270.0), (17.0, 0.0, 60.0),
+          (-75.0, 200.0, 12.5)]
+
+
+def test_rotation_matrix_matches_oracle():
+    import artiatomi_b200 as E
+    from oracle import geometry as G
+
+    table = {0, 30, 45, 60, 90, 120, 135, 150, 180, 210, 225, 240, 270, 300, 315, 330}
+    for a in ANGLES:
+        R = E.rotation_matrix(*a)
+        O = G.rotation_matrix(*a)
+        if all(float(x) in table for x in a):
+            np.testing.assert_array_equal(R, O)
+        else:
+            np.testing.assert_allclose(R, O, rtol=0, atol=3e-7)
+        np.testing.assert_allclose(R @ R.T, np.eye(3), atol=1e-6)
+    # exact table values where the reference uses them
+    np.testing.assert_array_equal(E.rotation_matrix(90.0, 0.0, 0.0), [[0, -1, 0], [1, 0, 0], [0, 0, 1]])
+
+
+def _orc_rotate(vol, R, q9=0):
+    from oracle import lib as OL
+
+    out = np.zeros_like(vol)
+    OL.olib.orc_rotate_volume(OL.addr(vol), OL.addr(out), vol.shape[0], OL.addr(np.ascontiguousarray(R, np.float32)),
+                              q9, OL.NTHREADS)
+    return out
+
+
+def test_oracle_rotation_pinned_to_reference_kernel():
+    from oracle import geometry as G
+    from oracle import lib as OL
+    from oracle import ref as RF
+
+    L = RF.lib()
+    if L is None:
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    rng = np.random.default_rng(4)
+    vol = rng.normal(size=(24, 24, 24)).astype(np.float32)
+    for a in ANGLES:
+        R = np.ascontiguousarray(G.rotation_matrix(*a), np.float32)
+        for q9 in (0, 1):
+            ref = np.zeros_like(vol)
+            assert L.ref_rot3d(OL.addr(vol), OL.addr(ref), 24, OL.addr(R), q9, OL.NTHREADS) == 0
+            np.testing.assert_array_equal(_orc_rotate(vol, R, q9), ref)
+
+
+REFINE_KEYS = """SizeSubVol = 16
+VoxelSizeSubVol = 1
+MotiveList = /data/motl.em
+Reference = /data/ref.em
+MaxShift = 3
+ShiftOutputFile = /data/shifts.em
+GroupMode = MaxCount
+GroupSize = 5
+SpeedUpDistance = 0
+ScaleMotivelistShift = 1
+ScaleMotivelistPosition = 1
+MultiPeakDetection = false
+"""
+
+
+def test_refine_config_keys():
+    from artiatomi_b200.config import EmSartConfig
+    from tests.test_fileio import CFG
+
+    c = EmSartConfig.from_text(CFG + REFINE_KEYS, refine=True)
+    assert c.Reference == "/data/ref.em" and c.ShiftOutputFile == "/data/shifts.em"
+    assert c.SizeSubVol == 16 and c.MaxShift == 3 and c.GroupMode == "MaxCount" and c.GroupSize == 5
+    assert not c.MultiPeakDetection
+    with pytest.raises(KeyError):  # required as in the reference (utils/Config.cpp:408-470)
+        EmSartConfig.from_text(CFG + REFINE_KEYS.replace("Reference = /data/ref.em\n", ""), refine=True)
+    with pytest.raises(ValueError):
+        EmSartConfig.from_text(CFG + REFINE_KEYS.replace("MaxCount", "Nearest"), refine=True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("size", [20, 32])
+def test_rotate_volume_matches_oracle(size):
+    import torch
+
+    import artiatomi_b200 as E
+
+    rng = np.random.default_rng(size)
+    vol = rng.normal(size=(size, size, size)).astype(np.float32)
+    src = cuda(vol)
+    out = torch.empty_like(src)
+    for a in ANGLES:
+        R = E.rotation_matrix(*a)
+        E.rotate_volume(src, out, R)
+        ref = _orc_rotate(vol, R)
+        # the kernel contracts the sample position into FMAs (~1 ulp of a
+        # coordinate ~10); on white noise that moves values by ~1e-6
+        assert rel_l2(host(out), ref) <= 1e-5, (a, rel_l2(host(out), ref))
+    with pytest.raises(Exception):
+        E.rotate_volume(src, src, E.rotation_matrix(10.0, 20.0, 30.0))  # in place is refused
+
+
+@pytest.mark.gpu
+def test_projection_loss_grad_roi_matches_full_image():
+    """A particle box whose shadow lies inside the region, measured zero
+    outside it: the region's 6 sums equal the whole image's, and the two
+    moments equal sum p^2 and sum p b of the projection."""
+    import torch
+
+    import artiatomi_b200 as E
+    from artiatomi_b200 import phantom as PH
+
+    W = H = 96
+    tilt = np.array([-35.0, 0.0, 50.0], np.float32)
+    pg = E.projection_geometry(E.Markers(tilt, rotation_psi=np.full(3, 12.0, np.float32)), W, H)
+    full = E.volume_geometry((96, 96, 32))
+    sub = E.subvolume_geometry(16, 1.0, full, (50.0, 44.0, 16.0))
+    box = cuda(PH.phantom_numpy((16, 16, 16), 4, seed=3))
+    rng = np.random.default_rng(0)
+    roi = (20, 16, 80, 76)
+    for i in range(3):
+        c = E.set_constant_values(pg[i], sub)
+        meas = np.zeros((H, W), np.float32)
+        meas[roi[1]:roi[3], roi[0]:roi[2]] = rng.normal(size=(roi[3] - roi[1], roi[2] - roi[0]))
+        m = cuda(meas)
+        o6 = torch.zeros(6, dtype=torch.float64, device="cuda")
+        o8 = torch.zeros(8, dtype=torch.float64, device="cuda")
+        p_full = torch.zeros((H, W), device="cuda")
+        p_roi = torch.full((H, W), 7.0, device="cuda")
+        E.projection_loss_grad(c, box, m, o6, shift=(0.3, -0.4), proj_out=p_full)
+        E.projection_loss_grad_roi(c, box, m, o8, roi, shift=(0.3, -0.4), proj_out=p_roi)
+        pf, pr = host(p_full), host(p_roi)
+        assert np.abs(pf).sum() > 0
+        outside = np.ones((H, W), bool)
+        outside[roi[1]:roi[3], roi[0]:roi[2]] = False
+        assert np.all(pf[outside] == 0.0)  # the shadow lies inside the region
+        assert np.all(pr[outside] == 7.0)  # pixels outside the region are not written
+        np.testing.assert_array_equal(pr[~outside], pf[~outside])
+        np.testing.assert_allclose(host(o8)[:6], host(o6), rtol=1e-9, atol=1e-12)
+        pd = pf.astype(np.float64)
+        np.testing.assert_allclose(host(o8)[6:], [(pd * pd).sum(), (pd * meas).sum()], rtol=1e-6)
+
+
+def _refine_dataset(tmp_path):
+    """Background phantom with the particle cubes zeroed, plus three rotated
+    references projected with known extra shifts; files as EmSart and
+    EmSartRefine read them."""
+    import torch
+
+    import artiatomi_b200 as E
+    from artiatomi_b200 import fileio as F
+    from artiatomi_b200 import phantom as PH
+
+    dims, W, H, n, S = (96, 96, 32), 128, 128, 5, 16
+    tilt = np.linspace(-40.0, 40.0, n).astype(np.float32)
+    psi = np.full(n, 8.0, np.float32)
+    markers = E.Markers(tilt, rotation_psi=psi)
+    pg = E.projection_geometry(markers, W, H)
+    vg = E.volume_geometry(dims)
+    rng = np.random.default_rng(7)
+    pos = np.array([[26.0, 28.0, 16.0], [70.0, 66.0, 17.0], [28.0, 70.0, 15.0]], np.float32)
+    angles = np.array([[10.0, 35.0, 70.0], [200.0, 15.0, 45.0], [0.0, 90.0, 30.0]], np.float32)
+    es = rng.uniform(-1.5, 1.5, size=(n, 3, 2)).astype(np.float32)  # [projection][motive][2]
+    back = PH.phantom_numpy(dims, 12, seed=2)
+    r = S // 2
+    for p in range(3):  # Volume::RemoveSubVolume's cube of each particle
+        lo = [int(pos[p, k]) - 1 - r for k in range(3)]
+        back[lo[2]:lo[2] + 2 * r, lo[1]:lo[1] + 2 * r, lo[0]:lo[0] + 2 * r] = 0.0
+    # a particle reference inside a spherical mask (zero near the box faces,
+    # so rotated and shifted copies read no clamped border voxels)
+    zz, yy, xx = np.mgrid[0:S, 0:S, 0:S] - (S // 2)
+    ref = (PH.phantom_numpy((S, S, S), 5, seed=11) * 4.0 * (xx ** 2 + yy ** 2 + zz ** 2 <= 36)).astype(np.float32)
+    ref_d = cuda(ref)
+    rot = torch.empty_like(ref_d)
+    back_d = cuda(back)
+    D = torch.zeros((n, H, W), device="cuda")
+    dist = torch.zeros((H, W), device="cuda")
+    for i in range(n):
+        E.forward_project(E.set_constant_values(pg[i], vg), back_d, D[i], dist, fast=True)
+    for p in range(3):
+        E.rotate_volume(ref_d, rot, E.rotation_matrix(*angles[p]))
+        sub = E.subvolume_geometry(S, 1.0, vg, pos[p], (0.0, 0.0, 0.0))
+        g = E.projection_geometry(markers, W, H, extra_shift=es[:, p, :])
+        for i in range(n):
+            E.forward_project(E.set_constant_values(g[i], sub), rot, D[i], dist, fast=True)
+    raw = (1000.0 - host(D)).astype(np.float32)
+    F.write_mrc(str(tmp_path / "ts.mrc"), raw, 0.5)
+    items = np.zeros((1, n, 10), np.float32)
+    items[0, :, 0], items[0, :, 1:3], items[0, :, 8], items[0, :, 9] = tilt, 10.0, 1.0, psi
+    F.write_markers(str(tmp_path / "markers.em"), items)
+    F.write_em(str(tmp_path / "vol.em"), -back)  # EmSart writes the volume negated
+    F.write_em(str(tmp_path / "ref.em"), ref)
+    motl = np.zeros((3, 20), np.float32)
+    motl[:, 3] = np.arange(1, 4)
+    motl[:, 7:10] = pos
+    motl[:, 16:19] = angles
+    F.write_motive_list(str(tmp_path / "motl.em"), motl)
+    cfg = f"""ProjectionFile = {tmp_path / 'ts.mrc'}
+OutVolumeFile = {tmp_path / 'vol.em'}
+MarkerFile = {tmp_path / 'markers.em'}
+Lambda = 1
+Iterations = 1
+RecDimesions = {dims[0]} {dims[1]} {dims[2]}
+UseFixPsiAngle = false
+PhiAngle = 0
+VolumeShift = 0 0 0
+ReferenceMarker = 0
+OverSampling = 1
+VoxelSize = 1
+DimLength = 1 1
+CutLength = 1 1
+SkipFilter = true
+fourFilterLP = 0
+fourFilterLPS = 0
+fourFilterHP = 0
+fourFilterHPS = 0
+SIRTCount = 1
+CtfMode = false
+BadPixelValue = 10
+CorrectBadPixels = false
+ProjectionNormalization = none
+WBP = false
+WBPFilter = Ramp
+SizeSubVol = {S}
+VoxelSizeSubVol = 1
+MotiveList = {tmp_path / 'motl.em'}
+Reference = {tmp_path / 'ref.em'}
+MaxShift = 3
+ShiftOutputFile = {tmp_path / 'shifts.em'}
+GroupMode = MaxCount
+GroupSize = 1
+SpeedUpDistance = 0
+ScaleMotivelistShift = 1
+ScaleMotivelistPosition = 1
+MultiPeakDetection = false
+"""
+    (tmp_path / "refine.cfg").write_text(cfg)
+    return es
+
+
+@pytest.mark.gpu
+def test_refine_recovers_extra_shifts(tmp_path):
+    """Every particle's per-tilt extra shift comes back within 0.05 px (the
+    data's rays start from the shifted detector, the fitted model translates
+    the unshifted rays' samples: their sample depths differ by up to a
+    step), and the ShiftFile written is the one EmSARTSubVolumes reads
+    (read_shift_file)."""
+    from artiatomi_b200 import fileio as F
+    from artiatomi_b200.config import EmSartConfig
+    from artiatomi_b200.refine import refine_shifts
+
+    es = _refine_dataset(tmp_path)
+    cfg = EmSartConfig.from_file(str(tmp_path / "refine.cfg"), refine=True)
+    got = refine_shifts(cfg)
+    assert got.shape == es.shape
+    err = np.abs(got - es).max()
+    assert err <= 5e-2, (err, got, es)
+    np.testing.assert_array_equal(F.read_shift_file(cfg.ShiftOutputFile), got)
