@@ -1,5 +1,5 @@
-// Reference kernels `wbpWeighting`, `fourierFilter`, `doseWeighting`
-// (wbpWeighting.cu), host-compiled.
+// Reference kernels `wbpWeighting`, `fourierFilter`, `doseWeighting` and
+// `rot3d` (wbpWeighting.cu), host-compiled.
 #include "ref_launch.h"
 namespace ref_wbp {
 ESB_REF_USING
