@@ -149,7 +149,7 @@ __device__ float cell_sum(const Cell<VT>& C, float qx, float qy, float qz, float
 //   sum_m f = M [f(a, c) + k5 da dc (M^2 - 1) / 12].
 // Samples are assigned to cells exactly as by the cell-by-cell DDA (the
 // sample parameter of each face crossing, rounded up).
-template <int VT, bool ZMAJ>
+template <int VT, bool ZMAJ, class Off>
 __device__ float layer_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float qz, float dqx, float dqz, int j0,
                               int J) {
   if (j0 >= J) return 0.0f;
@@ -169,22 +169,23 @@ __device__ float layer_sum_xz(const Cell<VT>& C, float qx, float b, int iy, floa
   float nNs = dN > 0.f ? ((fcn + 1.f) - pN) * isN : inf;
   const float g = dN * dM * (1.0f / 12.0f);
   const float jb = fj0 - 0.5f;
-  // 32-bit element offsets (volumes of up to 2^32 voxels; the launchers check)
-  const unsigned SM = ZMAJ ? (unsigned)C.sz : 1u, SN = ZMAJ ? 1u : (unsigned)C.sz;
+  // element offsets of type Off: 32-bit below 2^32 voxels (cheaper address
+  // arithmetic), 64-bit above (the launchers choose)
+  const Off SM = ZMAJ ? (Off)C.sz : (Off)1, SN = ZMAJ ? (Off)1 : (Off)C.sz;
   const int nMax = ZMAJ ? C.nz - 1 : C.nx - 1, nNax = ZMAJ ? C.nx - 1 : C.nz - 1;
-  auto clampM = [&](int i) { return (unsigned)(i < 0 ? 0 : (i > nMax ? nMax : i)) * SM; };
-  auto clampN = [&](int i) { return (unsigned)(i < 0 ? 0 : (i > nNax ? nNax : i)) * SN; };
-  const unsigned y0 = (unsigned)(iy < 0 ? 0 : (iy > C.ny - 1 ? C.ny - 1 : iy)) * (unsigned)C.sy;
-  const unsigned y1 = (unsigned)(iy + 1 < 0 ? 0 : (iy + 1 > C.ny - 1 ? C.ny - 1 : iy + 1)) * (unsigned)C.sy;
+  auto clampM = [&](int i) { return (Off)(i < 0 ? 0 : (i > nMax ? nMax : i)) * SM; };
+  auto clampN = [&](int i) { return (Off)(i < 0 ? 0 : (i > nNax ? nNax : i)) * SN; };
+  const Off y0 = (Off)(iy < 0 ? 0 : (iy > C.ny - 1 ? C.ny - 1 : iy)) * (Off)C.sy;
+  const Off y1 = (Off)(iy + 1 < 0 ? 0 : (iy + 1 > C.ny - 1 ? C.ny - 1 : iy + 1)) * (Off)C.sy;
   const float ib = 1.0f - b;
-  auto ey = [&](unsigned o) {
+  auto ey = [&](Off o) {
     return ib * Voxel<VT>::load(C.vol, (long)(o + y0)) + b * Voxel<VT>::load(C.vol, (long)(o + y1));
   };
   // original indices of the current cell's near and far corners per axis
   int inF = sn * (int)fcn + sn;
   int imF = sm * (int)fcm + sm;
-  unsigned on = clampN(inF - sn), of = clampN(inF);
-  unsigned omn = clampM(imF - sm), omf = clampM(imF);
+  Off on = clampN(inF - sn), of = clampN(inF);
+  Off omn = clampM(imF - sm), omf = clampM(imF);
   float enn = ey(on + omn), efn = ey(of + omn);
   const float Mt = (float)(J - j0);
   float fm0 = 0.0f, acc = 0.0f;
@@ -196,7 +197,7 @@ __device__ float layer_sum_xz(const Cell<VT>& C, float qx, float b, int iy, floa
     const float sA = fminf(nNs, nMs);
     const float fmA = fmaxf(sA >= Mt ? Mt : ceilf(sA), fm0);
     const int inF2 = inF + sn;
-    const unsigned o2 = clampN(inF2);
+    const Off o2 = clampN(inF2);
     const float enf = ey(on + omf), eff = ey(of + omf);
     const float e2n = ey(o2 + omn), e2f = ey(o2 + omf);
     {
@@ -236,16 +237,16 @@ __device__ float layer_sum_xz(const Cell<VT>& C, float qx, float b, int iy, floa
   return acc;
 }
 
-template <int VT>
+template <int VT, class Off>
 __device__ float cell_sum_xz(const Cell<VT>& C, float qx, float b, int iy, float qz, float dqx, float dqz, int j0,
                              int J) {
-  if (fabsf(dqz) >= fabsf(dqx)) return layer_sum_xz<VT, true>(C, qx, b, iy, qz, dqx, dqz, j0, J);
-  return layer_sum_xz<VT, false>(C, qx, b, iy, qz, dqx, dqz, j0, J);
+  if (fabsf(dqz) >= fabsf(dqx)) return layer_sum_xz<VT, true, Off>(C, qx, b, iy, qz, dqx, dqz, j0, J);
+  return layer_sum_xz<VT, false, Off>(C, qx, b, iy, qz, dqx, dqz, j0, J);
 }
 
 // Sum over the samples of one sub-ray from t0 to tout (first_at_source: the
 // slicer's first sample is taken at the ray start, ForwardProjectionSlicer.cu:126-141).
-template <int VT>
+template <int VT, class Off>
 __device__ float ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0, float tout, bool first_at_source) {
   const float h = c.vs.x * 0.15f;
   float step;
@@ -280,13 +281,13 @@ __device__ float ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0,
   const float ylast = qpos(q0.y, J - 1, dqy);
   if (fabsf(dqy) * (float)J < 1e-5f && floorf(q0.y) == floorf(ylast)) {
     const float fy = floorf(q0.y);
-    return sum + cell_sum_xz<VT>(C, q0.x, q0.y - fy, (int)fy, q0.z, dqx, dqz, j0, J);
+    return sum + cell_sum_xz<VT, Off>(C, q0.x, q0.y - fy, (int)fy, q0.z, dqx, dqz, j0, J);
   }
   return sum + cell_sum<VT>(C, q0.x, q0.y, q0.z, dqx, dqy, dqz, j0, J);
 }
 
 // mode 0: march (proj += sum/4, dist = mean chord); mode 1: slicer (proj += sum/4 within [tmin, tmax])
-template <int VT, int MODE>
+template <int VT, int MODE, class Off>
 __global__ void __launch_bounds__(128, 6) k_project_fast(KConst c, const void* __restrict__ vol, float* __restrict__ proj,
                                                       float* __restrict__ dist, size_t pitchE, float tminDef,
                                                       float tmaxDef, int x0, int y0, int x1, int y1) {
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(128, 6) k_project_fast(KConst c, const void* _
         tin = fmaxf(tin, tminDef);
         tout = fminf(tout, tmaxDef);
       }
-      sum = ray_sum<VT>(c, C, s, tin, tout, MODE == 1);
+      sum = ray_sum<VT, Off>(c, C, s, tin, tout, MODE == 1);
     }
   }
   sum = quad_sum_ordered(sum);
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(128, 6) k_project_fast(KConst c, const void* _
 // called once per slab by Reconstructor.cpp:515-585). The 4 lanes of a pixel
 // walk the union of their slab ranges together so each slab's sum keeps the
 // reference's sub-ray order.
-template <int VT>
+template <int VT, class Off>
 __global__ void __launch_bounds__(128, 6) k_slicer_fused(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
                                                       size_t img_stride, size_t pitchE, SlabTable slabs, int x0, int y0,
                                                       int x1, int y1) {
@@ -381,12 +382,15 @@ __global__ void __launch_bounds__(128, 6) k_slicer_fused(KConst c, const void* _
     if (hitray && k >= klo && k <= khi) {
       const float t0 = fmaxf(tin, slabs.bound[k]);
       const float t1 = fminf(tout, slabs.bound[k + 1]);
-      v = ray_sum<VT>(c, C, s, t0, t1, true);
+      v = ray_sum<VT, Off>(c, C, s, t0, t1, true);
     }
     v = quad_sum_ordered(v);
     if (active && sub == 0 && k >= klo && k <= khi) imgs[(size_t)k * img_stride + pix] = v * c.vs.x * 0.15f * 0.25f;
   }
 }
+
+// Volumes of 2^32 voxels or more take 64-bit element offsets in the walk.
+bool big_volume(const KConst& c) { return (double)c.dim.x * c.dim.y * c.dim.z > 4294967295.0; }
 
 }  // namespace
 
@@ -394,14 +398,19 @@ cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float*
                                 size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1,
                                 cudaStream_t st) {
   if (x1 <= x0 || y1 <= y0 || slabs.count <= 0) return cudaSuccess;
-  if ((double)c.dim.x * c.dim.y * c.dim.z > 4294967295.0) return cudaErrorInvalidValue;  // 32-bit voxel offsets
   dim3 blk(128), grd((x1 - x0 + 3) / 4, (y1 - y0 + 7) / 8);
-  if (vt == ESB_VOXEL_F32)
-    k_slicer_fused<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
-  else if (vt == ESB_VOXEL_F16)
-    k_slicer_fused<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
-  else
-    k_slicer_fused<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
+#define ESB_LAUNCH(VT, OFF) \
+  k_slicer_fused<VT, OFF><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1)
+  if (big_volume(c)) {
+    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, unsigned long long);
+    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, unsigned long long);
+    else ESB_LAUNCH(ESB_VOXEL_BF16, unsigned long long);
+  } else {
+    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, unsigned);
+    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, unsigned);
+    else ESB_LAUNCH(ESB_VOXEL_BF16, unsigned);
+  }
+#undef ESB_LAUNCH
   ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
@@ -410,22 +419,27 @@ cudaError_t launch_project_fast(const KConst& c, const void* vol, int vt, int mo
                                 size_t pitchE, float tmin, float tmax, int x0, int y0, int x1, int y1,
                                 cudaStream_t st) {
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
-  if ((double)c.dim.x * c.dim.y * c.dim.z > 4294967295.0) return cudaErrorInvalidValue;  // 32-bit voxel offsets
   dim3 blk(128), grd((x1 - x0 + 3) / 4, (y1 - y0 + 7) / 8);
-#define ESB_LAUNCH(VT, M)                                                                            \
-  do {                                                                                               \
-    k_project_fast<VT, M><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, tmin, tmax, x0, y0, x1, y1); \
-    ESB_COUNT_LAUNCH();                                                                              \
+#define ESB_LAUNCH(VT, M, OFF)                                                                            \
+  do {                                                                                                    \
+    k_project_fast<VT, M, OFF><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, tmin, tmax, x0, y0, x1, y1); \
+    ESB_COUNT_LAUNCH();                                                                                   \
   } while (0)
+#define ESB_LAUNCH_VT(M, OFF)                         \
+  do {                                                \
+    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, M, OFF);   \
+    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, M, OFF); \
+    else ESB_LAUNCH(ESB_VOXEL_BF16, M, OFF);          \
+  } while (0)
+  const bool big = big_volume(c);
   if (mode == 0) {
-    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, 0);
-    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, 0);
-    else ESB_LAUNCH(ESB_VOXEL_BF16, 0);
+    if (big) ESB_LAUNCH_VT(0, unsigned long long);
+    else ESB_LAUNCH_VT(0, unsigned);
   } else {
-    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, 1);
-    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, 1);
-    else ESB_LAUNCH(ESB_VOXEL_BF16, 1);
+    if (big) ESB_LAUNCH_VT(1, unsigned long long);
+    else ESB_LAUNCH_VT(1, unsigned);
   }
+#undef ESB_LAUNCH_VT
 #undef ESB_LAUNCH
   return cudaGetLastError();
 }

@@ -210,3 +210,51 @@ def test_subvolume_wbp_rotated_axis(ctf):
         assert rel_l2(b, a) <= 1e-5, rel_l2(b, a)
         tol = max(1e-4 if not ctf else 1e-3, 1.5 * rel_l2(r32, r64))
         assert rel_l2(b, r64) <= tol, (rel_l2(b, r64), tol)
+
+
+@pytest.mark.gpu
+def test_fast_projection_of_a_volume_above_2_32_voxels():
+    """A 1024 x 4100 x 1024 FP16 volume (4.3e9 voxels, 8.6 GB) with content in
+    an 8-plane y band only: single-axis rays stay in one y plane, so the
+    projection of the detector columns over the band equals that of the
+    band alone (its own 1024 x 8 x 1024 volume at the same place). The walk
+    then takes 64-bit element offsets."""
+    import ctypes as C
+
+    import torch
+
+    import artiatomi_b200 as E
+
+    X, Y, Z, yb = 1024, 4100, 1024, 4088
+    assert X * Y * Z > 2 ** 32
+    W, H = 4100, 1600
+    tilt = np.array([-50.0, 0.0, 35.0], np.float32)
+    pg = E.projection_geometry(E.Markers(tilt), W, H)
+    vg = E.volume_geometry((X, Y, Z))
+    band = torch.randn((Z, 8, X), device="cuda").half()
+    big = torch.zeros((Z, Y, X), dtype=torch.float16, device="cuda")
+    big[:, yb:yb + 8, :] = band
+    # the band's own volume geometry: vg cut to y planes [yb, yb + 8)
+    bg = E.volume_geometry((X, Y, Z))
+    vs = float(vg.voxel_size[1])
+    bg.bbox_min[1] = vg.bbox_min[1] + yb * vs
+    bg.bbox_max[1] = bg.bbox_min[1] + 8 * vs
+    bg.dim[1] = 8.0
+    bg.bbox_rcp[1] = 1.0 / (8 * vs)
+    for i in range(len(tilt)):
+        cb = E.set_constant_values(pg[i], vg)
+        cs = E.set_constant_values(pg[i], bg)
+        # detector columns whose rays cross the band's interior planes
+        u = [int(np.floor(np.dot(np.array(cb.detector_matrix[0:3]), [0.0, vg.bbox_min[1] + (yb + k) * vs, 0.0])
+                          + cb.detector_matrix[3])) for k in (2, 6)]
+        roi = (min(u), 0, max(u), H)
+        outs = []
+        for vol, c in ((big, cb), (band.contiguous(), cs)):
+            proj = torch.zeros((H, W), device="cuda")
+            dist = torch.zeros((H, W), device="cuda")
+            E.forward_project(c, vol, proj, dist, roi=roi, fast=True)
+            outs.append(host(proj)[:, roi[0]:roi[2]])
+        assert np.abs(outs[1]).sum() > 0
+        assert rel_l2(outs[0], outs[1]) <= 1e-3, (i, rel_l2(outs[0], outs[1]))
+    del big
+    torch.cuda.empty_cache()
