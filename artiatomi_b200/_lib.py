@@ -98,6 +98,8 @@ _SIGS = {
     "esb_projection_loss_grad": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, F, P, P, P, P], I),
     "esb_projection_loss_grad_roi": ([C.POINTER(Constants), P, I, I, I, P, SZ, F, F, P, P, P, P, P], I),
     "esb_rotation_matrix": ([F, F, F, P], I),
+    "esb_autotune": ([I], I),
+    "esb_autotune_report": ([C.c_char_p, SZ, C.POINTER(SZ)], I),
     "esb_rotate_volume": ([P, P, I, P, P], I),
     "esb_make_square": ([I, I, SZ, P, I, P, I, I, I, I, P], I),
     "esb_ctf": ([P, I, F, F, F, I, I, F, P, F, F, F, F, P], I),

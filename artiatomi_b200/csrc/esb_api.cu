@@ -2,13 +2,17 @@
 // and the Reconstructor (buffers, cuFFT plans, CTF slab loops, SART driver
 // loop, sub-volume back-projection).
 #include <cufft.h>
+#include <float.h>
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "esb_device.cuh"
@@ -25,18 +29,19 @@ cudaError_t launch_travlen(const KConst& c, float* dist, size_t pitchE, int x0, 
 cudaError_t launch_bp(const KConst& c, void* vol, int vt, const float* img, int pw, int ph, size_t pitchE, float lambda,
                       int os, float distMin, float distMax, int linear, cudaStream_t st);
 cudaError_t launch_project_fast(const KConst& c, const void* vol, int vt, int mode, float* proj, float* dist,
-                                size_t pitchE, float tmin, float tmax, int x0, int y0, int x1, int y1, cudaStream_t st);
+                                size_t pitchE, float tmin, float tmax, int x0, int y0, int x1, int y1, cudaStream_t st, int nw = 4);
 cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img, int pw, int ph, size_t pitchE,
                            float lambda, int os, float distMin, float distMax, int linear, cudaStream_t st);
 cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
                                  const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
                                  float distMin, float distMax, int linear, cudaStream_t st, int transposed,
-                                 const float* ups = nullptr, size_t up_stride = 0);
+                                 const float* ups = nullptr, size_t up_stride = 0, const BpShape* shape = nullptr);
 cudaError_t launch_upsample(const float* imgs, size_t img_stride, int count, int pw, int ph, int os, int linear,
                             float* up, size_t up_stride, cudaStream_t st);
 bool bp_can_upsample(const KConst& k, int os);
+bool bp_uses_axis(const KConst& k, int os);
 cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float* imgs, size_t img_stride,
-                                size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1, cudaStream_t st);
+                                size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1, cudaStream_t st, int nw = 4);
 cudaError_t launch_compare(int pw, int ph, size_t pitchE, const float* real, float* virt, const float* dist,
                            float realLength, float4 cut, float4 dim, float scale, cudaStream_t st);
 cudaError_t launch_crop_border(int pw, int ph, size_t pitchE, float* img, float2 cut, float2 dim, const int* p,
@@ -429,6 +434,8 @@ struct esb_reconstructor {
   size_t slab_cap = 0;         // capacity in images
   float* up_imgs = nullptr;    // the slab images pre-sampled on the sub-pixel grid
   size_t up_cap = 0;           // capacity in floats
+  void* tune_scratch = nullptr;  // the autotuner's trial outputs
+  size_t tune_cap = 0;           // capacity in bytes
   SubvolBatch batch;           // tables of the batched sub-volume launch
   // filtered spectra and squares of a chunk of CTF slabs, with a batched
   // C2R plan per chunk size
@@ -499,6 +506,7 @@ static void rec_free(esb_reconstructor* r) {
   r->slab_imgs = nullptr;
   r->slab_cap = 0;
   cudaFree(r->up_imgs);
+  cudaFree(r->tune_scratch);
   r->up_imgs = nullptr;
   r->up_cap = 0;
   subvol_batch_free(r->batch);
@@ -647,11 +655,196 @@ int esb_rec_reset_projections(esb_reconstructor* r) {
 
 }  // extern "C"
 
+// ------------------------------------------------------------ autotuning
+// Launch shapes that do not change results (every thread does the same work
+// under every shape) are picked per GPU and problem shape the first time a
+// reconstructor launches the kernel outside stream capture: each candidate
+// is timed with CUDA events on the reconstructor's stream (one warm-up
+// launch, two timed ones) and the fastest is cached for the process.
+// Projector candidates read the real volume and write scratch images;
+// back-projection candidates run on a 16-plane scratch slab from the middle
+// of the volume, so the caller's volume is never written by a trial. During
+// capture, or when tuning is off, the cached or the default shape is taken.
+namespace {
+struct TuneKey {
+  int kernel, dev, sms, vt, w, h, dx, dy, dz, os, ctf;
+  auto tie() const { return std::tie(kernel, dev, sms, vt, w, h, dx, dy, dz, os, ctf); }
+  bool operator<(const TuneKey& o) const { return tie() < o.tie(); }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+std::atomic<int> g_tune_on{1};
+std::atomic<int> g_tune_force{-1};  // >= 0: every tuned kernel takes this candidate (tests)
+// back-projection shapes (quads x rows per block), candidate index -> shape
+const int kBpShapes[][2] = {{32, 4}, {32, 2}, {16, 8}, {64, 2}, {32, 1}};
+const int kNBpShapes = 5;
+const char* kTuneNames[] = {"fp_slicer_fused", "fp_march", "bp_axis"};
+}  // namespace
+
+static TuneKey tune_key(esb_reconstructor* r, int kernel, int vt, const KConst& c, int ctf) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return TuneKey{kernel, dev, sms, vt, r->cfg.proj_x, r->cfg.proj_y, (int)c.dim.x, (int)c.dim.y, (int)c.dim.z,
+                 r->cfg.oversampling, ctf};
+}
+
+static void* rec_tune_scratch(esb_reconstructor* r, size_t bytes) {
+  if (bytes <= r->tune_cap) return r->tune_scratch;
+  if (cudaStreamSynchronize(r->stream) != cudaSuccess) return nullptr;
+  cudaFree(r->tune_scratch);
+  r->tune_scratch = nullptr;
+  r->tune_cap = 0;
+  if (cudaMalloc(&r->tune_scratch, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  r->tune_cap = bytes;
+  return r->tune_scratch;
+}
+
+// The cached choice for key, else candidates[0..n) timed with run(choice)
+// (a trial that fails excludes its candidate); def when nothing is measured.
+template <class Run>
+static int rec_tuned(esb_reconstructor* r, const TuneKey& key, int n, int def, Run run) {
+  const int forced = g_tune_force.load();
+  if (forced >= 0) return std::min(forced, n - 1);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+  }
+  if (!g_tune_on.load()) return def;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(r->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return def;
+  }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return def;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return def;
+  }
+  int best = def;
+  float best_ms = FLT_MAX;
+  for (int i = 0; i < n; ++i) {
+    if (run(i) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaEventRecord(e0, r->stream);
+    cudaError_t e = run(i);
+    if (e == cudaSuccess) e = run(i);
+    cudaEventRecord(e1, r->stream);
+    float ms = FLT_MAX;
+    if (e == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaGetLastError();
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune[key] = best;
+  return best;
+}
+
+static const int kNw[3] = {4, 2, 8};  // warps per projector block; index 0 is the default
+
+extern "C" int esb_autotune(int enable) {
+  if (enable < -1) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_autotune: enable must be >= -1");
+  if (enable == -1) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune.clear();
+  } else if (enable >= 2) {
+    g_tune_force.store(enable - 2);
+  } else {
+    g_tune_force.store(-1);
+    g_tune_on.store(enable);
+  }
+  return ok();
+}
+
+extern "C" int esb_autotune_report(char* buf, size_t len, size_t* needed) {
+  if (!buf && len) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_autotune_report: buf is NULL");
+  std::string text;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (const auto& kv : g_tune) {
+      const TuneKey& k = kv.first;
+      char line[256];
+      if (k.kernel == 2)
+        snprintf(line, sizeof line, "%s dev=%d sms=%d voxel=%d detector=%dx%d volume=%dx%dx%d os=%d ctf=%d block=%dx%d\n",
+                 kTuneNames[k.kernel], k.dev, k.sms, k.vt, k.w, k.h, k.dx, k.dy, k.dz, k.os, k.ctf,
+                 kBpShapes[kv.second][0], kBpShapes[kv.second][1]);
+      else
+        snprintf(line, sizeof line, "%s dev=%d sms=%d voxel=%d detector=%dx%d volume=%dx%dx%d os=%d ctf=%d warps=%d\n",
+                 kTuneNames[k.kernel], k.dev, k.sms, k.vt, k.w, k.h, k.dx, k.dy, k.dz, k.os, k.ctf, kNw[kv.second]);
+      text += line;
+    }
+  }
+  if (needed) *needed = text.size() + 1;
+  if (len) {
+    const size_t n = std::min(len - 1, text.size());
+    memcpy(buf, text.data(), n);
+    buf[n] = 0;
+  }
+  return ok();
+}
+
+// Warps per block of the fused slicer for this problem.
+static int rec_slicer_nw(esb_reconstructor* r, const KConst& c, const void* vol, int vt, size_t img,
+                         const SlabTable& T) {
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y;
+  const int i = rec_tuned(r, tune_key(r, 0, vt, c, 1), 3, 0, [&](int k) {
+    return launch_slicer_fused(c, vol, vt, r->slab_imgs, img, W, T, 0, 0, W, H, r->stream, kNw[k]);
+  });
+  return kNw[i];
+}
+
+// Warps per block of the march projector (trials write scratch images: the
+// projection accumulates into proj_d).
+static int rec_march_nw(esb_reconstructor* r, const KConst& c, const void* vol, int vt) {
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y;
+  const size_t img = (size_t)W * H;
+  const int i = rec_tuned(r, tune_key(r, 1, vt, c, 0), 3, 0, [&](int k) {
+    float* s = (float*)rec_tune_scratch(r, 2 * img * sizeof(float));
+    if (!s) return cudaErrorMemoryAllocation;
+    return launch_project_fast(c, vol, vt, 0, s, s + img, W, 0.f, 0.f, 0, 0, W, H, r->stream, kNw[k]);
+  });
+  return kNw[i];
+}
+
+// Block shape of the single-axis back-projection for this problem; trials on
+// a scratch slab of up to 16 planes from the middle of the volume.
+static BpShape rec_bp_shape(esb_reconstructor* r, const KConst& c, int vt, const float* imgs, size_t img_stride,
+                            const SlabTable& T, int linear, const float* up, size_t up_stride) {
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y, os = r->cfg.oversampling;
+  BpShape s{kBpShapes[0][0], kBpShapes[0][1], 0, 0};
+  if (!bp_uses_axis(c, os)) return s;
+  const int nz = (int)c.dim.z, planes = std::min(nz, 16);
+  const size_t plane = (size_t)c.dim.x * (size_t)c.dim.y * (vt == ESB_VOXEL_F32 ? 4 : 2);
+  const int i = rec_tuned(r, tune_key(r, 2, vt, c, T.count > 0), kNBpShapes, 0, [&](int k) {
+    void* slab = rec_tune_scratch(r, plane * planes);
+    if (!slab) return cudaErrorMemoryAllocation;
+    const BpShape t{kBpShapes[k][0], kBpShapes[k][1], std::max(0, nz / 2 - planes / 2), planes};
+    return launch_bp_fast_slabs(c, slab, vt, imgs, img_stride, T, W, H, W, 0.0f, os, 0.0f, 9999999999999.0f, linear,
+                                r->stream, 1, up, up_stride, &t);
+  });
+  s.bx = kBpShapes[i][0];
+  s.by = kBpShapes[i][1];
+  return s;
+}
+
 // Kernel variant of the reconstructor (faithful or fast).
 static cudaError_t rec_march(esb_reconstructor* r, const KConst& c, const void* vol, int vt) {
   const int W = r->cfg.proj_x, H = r->cfg.proj_y;
   if (r->cfg.variant == ESB_VARIANT_FAST)
-    return launch_project_fast(c, vol, vt, 0, r->proj_d, r->dist_d, W, 0.f, 0.f, 0, 0, W, H, r->stream);
+    return launch_project_fast(c, vol, vt, 0, r->proj_d, r->dist_d, W, 0.f, 0.f, 0, 0, W, H, r->stream,
+                               rec_march_nw(r, c, vol, vt));
   return launch_march(c, vol, vt, r->proj_d, r->dist_d, W, 0, 0, W, H, r->stream);
 }
 static cudaError_t rec_slicer(esb_reconstructor* r, const KConst& c, const void* vol, int vt, float* out, float t0,
@@ -915,7 +1108,8 @@ int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, con
     }
     {
       PhaseScope ps(r, 0);
-      ESB_CK(launch_slicer_fused(c, vol, voxel_type, r->slab_imgs, img, W, T, 0, 0, W, H, r->stream),
+      const int nw = rec_slicer_nw(r, c, vol, voxel_type, img, T);
+      ESB_CK(launch_slicer_fused(c, vol, voxel_type, r->slab_imgs, img, W, T, 0, 0, W, H, r->stream, nw),
              "esb_rec_forward_projection");
     }
     // each slab image through the CTF, added to proj_d in slab order
@@ -993,8 +1187,9 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
       size_t up_stride = 0;
       const float* up = rec_upsample(r, c, 1, 0, up_stride);
       ESB_CK(cudaGetLastError(), "back projection");
+      const BpShape shape = rec_bp_shape(r, c, voxel_type, r->slab_imgs, 0, none, 0, up, up_stride);
       ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, 0, none, W, H, W, lambda, cf.oversampling, 0.0f,
-                                  9999999999999.0f, 0, r->stream, 1, up, up_stride), "back projection");
+                                  9999999999999.0f, 0, r->stream, 1, up, up_stride, &shape), "back projection");
       return ESB_OK;
     }
     PhaseScope ps(r, 1);
@@ -1017,9 +1212,9 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
     size_t up_stride = 0;
     const float* up = rec_upsample(r, c, T.count, 1, up_stride);
     ESB_CK(cudaGetLastError(), "back projection");
+    const BpShape shape = rec_bp_shape(r, c, voxel_type, r->slab_imgs, (size_t)W * H, T, 1, up, up_stride);
     ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, (size_t)W * H, T, W, H, W, lambda, cf.oversampling,
-                                0.f, 0.f,
-                                1, r->stream, 1, up, up_stride), "back projection");
+                                0.f, 0.f, 1, r->stream, 1, up, up_stride, &shape), "back projection");
     return ESB_OK;
   }
   for (float ray = t_in; ray < t_out; ray += step) {

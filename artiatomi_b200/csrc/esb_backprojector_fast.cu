@@ -85,10 +85,13 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
                                                  const float* __restrict__ imgs, size_t img_stride, SlabTable slabs,
                                                  int pw, int ph, size_t pitchE, float lambda, int os, float inv,
                                                  float distMin, float distMax, int linear, int transposed,
-                                                 const float* __restrict__ ups, size_t up_stride) {
+                                                 const float* __restrict__ ups, size_t up_stride, int z0) {
+  // plane z0 + blockIdx.z of the geometry, stored at plane blockIdx.z of vol
+  // (z0 = 0 but for the autotuner's trial launches on a scratch slab)
   const int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
-  const int z = (int)blockIdx.z;
+  const int zl = (int)blockIdx.z;
+  const int z = z0 + zl;
   const int ny = (int)k.dim.y, nz = (int)k.dim.z;
   if (q >= k.dimXQuarter || y >= ny || z >= nz) return;
   const int x = 4 * q;
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
     const float px = ((float)mu + 0.5f) * inv, py = ((float)mv + 0.5f) * inv;
     return interior ? sample_interior(img, sx, sy, px, py, lin) : sample_image(img, pw, ph, pitchE, px, py, lin, tr);
   };
-  const long base = ((long)z * ny + y) * (long)k.dim.x + x;
+  const long base = ((long)zl * ny + y) * (long)k.dim.x + x;
   float res[4], has[4];
   const bool patch = !UP && os == 2 && lin && interior;
 #pragma unroll
@@ -176,7 +179,7 @@ __global__ void __launch_bounds__(256) k_upsample(const float* __restrict__ imgs
 cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
                                  const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
                                  float distMin, float distMax, int linear, cudaStream_t st, int transposed,
-                                 const float* ups, size_t up_stride) {
+                                 const float* ups, size_t up_stride, const BpShape* shape) {
   const int nq = k.dimXQuarter, ny = (int)k.dim.y, nz = (int)k.dim.z;
   if (nq <= 0 || ny <= 0 || nz <= 0) return cudaSuccess;
   const BpGeom g = make_geom(k, os);
@@ -184,9 +187,16 @@ cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float
   dim3 blk(32, 4, 1), grd((nq + 31) / 32, (ny + 3) / 4, nz);
   if (axis_eligible(k, g)) {
     const AxisGeom a = make_axis_geom(k, g, os);
+    int z0 = 0;
+    if (shape) {  // block of bx quads x by rows (bx * by <= 128); planes [z0, z0 + nz)
+      blk = dim3(shape->bx, shape->by, 1);
+      z0 = shape->z0;
+      grd = dim3((nq + shape->bx - 1) / shape->bx, (ny + shape->by - 1) / shape->by,
+                 shape->nz > 0 ? shape->nz : nz - z0);
+    }
 #define ESB_AXIS(VT, UP)                                                                                          \
   k_bp_axis<VT, UP><<<grd, blk, 0, st>>>(k, a, vol, imgs, img_stride, slabs, pw, ph, pitchE, lambda, os, inv, distMin, \
-                                         distMax, linear, transposed, ups, up_stride)
+                                         distMax, linear, transposed, ups, up_stride, z0)
     if (ups) {
       if (vt == ESB_VOXEL_F32) ESB_AXIS(ESB_VOXEL_F32, true);
       else if (vt == ESB_VOXEL_F16) ESB_AXIS(ESB_VOXEL_F16, true);
@@ -213,7 +223,7 @@ cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img,
   SlabTable none;
   none.count = 0;
   return launch_bp_fast_slabs(k, vol, vt, img, 0, none, pw, ph, pitchE, lambda, os, distMin, distMax, linear, st, 0,
-                              nullptr, 0);
+                              nullptr, 0, nullptr);
 }
 
 // Pre-sampled slab images for k_bp_fast (transposed input images, up_stride
@@ -234,5 +244,9 @@ bool bp_can_upsample(const KConst& k, int os) {
   const BpGeom g = make_geom(k, os);
   return g.exact_grid && g.aniso_identity;
 }
+
+// Whether launch_bp_fast_slabs takes the single-axis kernel (whose launch
+// shape BpShape sets).
+bool bp_uses_axis(const KConst& k, int os) { return axis_eligible(k, make_geom(k, os)); }
 
 }  // namespace esb

@@ -60,6 +60,13 @@ struct CtfConst {
   float cs, lambda, ampC, phaseC, freqStep, pixelcount;
 };
 
+// Launch shape of the single-axis back-projection: blocks of bx quads x by
+// rows (bx * by <= 128), over volume planes [z0, z0 + nz) (nz = 0: to the
+// end) written from plane 0 of the buffer passed.
+struct BpShape {
+  int bx, by, z0, nz;
+};
+
 // Every kernel launch of the library is counted (esb_kernel_launches).
 void count_launch();
 #define ESB_COUNT_LAUNCH() ::esb::count_launch()

@@ -287,18 +287,20 @@ __device__ float ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0,
 }
 
 // mode 0: march (proj += sum/4, dist = mean chord); mode 1: slicer (proj += sum/4 within [tmin, tmax])
-template <int VT, int MODE, class Off>
-__global__ void __launch_bounds__(128, 6) k_project_fast(KConst c, const void* __restrict__ vol, float* __restrict__ proj,
+// NW warps per block: NW detector columns x 8 rows; blocks of 128 threads
+// fit 6 per SM at the walker's register count (256-thread blocks fit 3); the
+// launch shape is picked per problem by the reconstructor's autotuner.
+template <int VT, int MODE, class Off, int NW>
+__global__ void __launch_bounds__(32 * NW, 24 / NW) k_project_fast(KConst c, const void* __restrict__ vol, float* __restrict__ proj,
                                                       float* __restrict__ dist, size_t pitchE, float tminDef,
                                                       float tmaxDef, int x0, int y0, int x1, int y1) {
   // lanes: 4 sub-rays of a pixel adjacent; a warp spans 8 detector rows (v);
-  // 4 warps per block: 4 detector columns (u). Blocks of 128 threads fit 6
-  // per SM at the walker's register count, where 256-thread blocks fit 3.
+  // the NW warps of a block, NW detector columns (u)
   const int lane = threadIdx.x & 31;
   const int sub = lane & 3;
   const int row = (threadIdx.x >> 2) & 7;
   const int warp = threadIdx.x >> 5;
-  const int x = x0 + (int)blockIdx.x * 4 + warp;
+  const int x = x0 + (int)blockIdx.x * NW + warp;
   const int y = y0 + (int)blockIdx.y * 8 + row;
   const bool active = x < x1 && y < y1;
   Cell<VT> C{vol, (int)c.dim.x, (int)c.dim.y, (int)c.dim.z, (long)c.dim.x, (long)c.dim.x * (long)c.dim.y};
@@ -335,15 +337,15 @@ __global__ void __launch_bounds__(128, 6) k_project_fast(KConst c, const void* _
 // called once per slab by Reconstructor.cpp:515-585). The 4 lanes of a pixel
 // walk the union of their slab ranges together so each slab's sum keeps the
 // reference's sub-ray order.
-template <int VT, class Off>
-__global__ void __launch_bounds__(128, 6) k_slicer_fused(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
+template <int VT, class Off, int NW>
+__global__ void __launch_bounds__(32 * NW, 24 / NW) k_slicer_fused(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
                                                       size_t img_stride, size_t pitchE, SlabTable slabs, int x0, int y0,
                                                       int x1, int y1) {
   const int lane = threadIdx.x & 31;
   const int sub = lane & 3;
   const int row = (threadIdx.x >> 2) & 7;
   const int warp = threadIdx.x >> 5;
-  const int x = x0 + (int)blockIdx.x * 4 + warp;
+  const int x = x0 + (int)blockIdx.x * NW + warp;
   const int y = y0 + (int)blockIdx.y * 8 + row;
   const bool active = x < x1 && y < y1;
   Cell<VT> C{vol, (int)c.dim.x, (int)c.dim.y, (int)c.dim.z, (long)c.dim.x, (long)c.dim.x * (long)c.dim.y};
@@ -394,22 +396,27 @@ bool big_volume(const KConst& c) { return (double)c.dim.x * c.dim.y * c.dim.z > 
 
 }  // namespace
 
+// nw: warps per block (2, 4 or 8; 64-bit-offset volumes always take 4).
 cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float* imgs, size_t img_stride,
                                 size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1,
-                                cudaStream_t st) {
+                                cudaStream_t st, int nw) {
   if (x1 <= x0 || y1 <= y0 || slabs.count <= 0) return cudaSuccess;
-  dim3 blk(128), grd((x1 - x0 + 3) / 4, (y1 - y0 + 7) / 8);
-#define ESB_LAUNCH(VT, OFF) \
-  k_slicer_fused<VT, OFF><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1)
-  if (big_volume(c)) {
-    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, unsigned long long);
-    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, unsigned long long);
-    else ESB_LAUNCH(ESB_VOXEL_BF16, unsigned long long);
-  } else {
-    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, unsigned);
-    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, unsigned);
-    else ESB_LAUNCH(ESB_VOXEL_BF16, unsigned);
-  }
+  const bool big = big_volume(c);
+  if (big || (nw != 2 && nw != 8)) nw = 4;
+  dim3 blk(32 * nw), grd((x1 - x0 + nw - 1) / nw, (y1 - y0 + 7) / 8);
+#define ESB_LAUNCH(VT, OFF, NW) \
+  k_slicer_fused<VT, OFF, NW><<<grd, blk, 0, st>>>(c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1)
+#define ESB_LAUNCH_VT(OFF, NW)                                  \
+  do {                                                          \
+    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, OFF, NW);   \
+    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, OFF, NW); \
+    else ESB_LAUNCH(ESB_VOXEL_BF16, OFF, NW);                   \
+  } while (0)
+  if (big) ESB_LAUNCH_VT(unsigned long long, 4);
+  else if (nw == 2) ESB_LAUNCH_VT(unsigned, 2);
+  else if (nw == 8) ESB_LAUNCH_VT(unsigned, 8);
+  else ESB_LAUNCH_VT(unsigned, 4);
+#undef ESB_LAUNCH_VT
 #undef ESB_LAUNCH
   ESB_COUNT_LAUNCH();
   return cudaGetLastError();
@@ -417,30 +424,32 @@ cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float*
 
 cudaError_t launch_project_fast(const KConst& c, const void* vol, int vt, int mode, float* proj, float* dist,
                                 size_t pitchE, float tmin, float tmax, int x0, int y0, int x1, int y1,
-                                cudaStream_t st) {
+                                cudaStream_t st, int nw) {
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
-  dim3 blk(128), grd((x1 - x0 + 3) / 4, (y1 - y0 + 7) / 8);
-#define ESB_LAUNCH(VT, M, OFF)                                                                            \
-  do {                                                                                                    \
-    k_project_fast<VT, M, OFF><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, tmin, tmax, x0, y0, x1, y1); \
-    ESB_COUNT_LAUNCH();                                                                                   \
-  } while (0)
-#define ESB_LAUNCH_VT(M, OFF)                         \
-  do {                                                \
-    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, M, OFF);   \
-    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, M, OFF); \
-    else ESB_LAUNCH(ESB_VOXEL_BF16, M, OFF);          \
-  } while (0)
   const bool big = big_volume(c);
-  if (mode == 0) {
-    if (big) ESB_LAUNCH_VT(0, unsigned long long);
-    else ESB_LAUNCH_VT(0, unsigned);
-  } else {
-    if (big) ESB_LAUNCH_VT(1, unsigned long long);
-    else ESB_LAUNCH_VT(1, unsigned);
-  }
+  if (big || (nw != 2 && nw != 8)) nw = 4;
+  dim3 blk(32 * nw), grd((x1 - x0 + nw - 1) / nw, (y1 - y0 + 7) / 8);
+#define ESB_LAUNCH(VT, M, OFF, NW) \
+  k_project_fast<VT, M, OFF, NW><<<grd, blk, 0, st>>>(c, vol, proj, dist, pitchE, tmin, tmax, x0, y0, x1, y1)
+#define ESB_LAUNCH_VT(M, OFF, NW)                                  \
+  do {                                                             \
+    if (vt == ESB_VOXEL_F32) ESB_LAUNCH(ESB_VOXEL_F32, M, OFF, NW);   \
+    else if (vt == ESB_VOXEL_F16) ESB_LAUNCH(ESB_VOXEL_F16, M, OFF, NW); \
+    else ESB_LAUNCH(ESB_VOXEL_BF16, M, OFF, NW);                   \
+  } while (0)
+#define ESB_LAUNCH_NW(M)                                      \
+  do {                                                        \
+    if (big) ESB_LAUNCH_VT(M, unsigned long long, 4);          \
+    else if (nw == 2) ESB_LAUNCH_VT(M, unsigned, 2);           \
+    else if (nw == 8) ESB_LAUNCH_VT(M, unsigned, 8);           \
+    else ESB_LAUNCH_VT(M, unsigned, 4);                        \
+  } while (0)
+  if (mode == 0) ESB_LAUNCH_NW(0);
+  else ESB_LAUNCH_NW(1);
+#undef ESB_LAUNCH_NW
 #undef ESB_LAUNCH_VT
 #undef ESB_LAUNCH
+  ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 

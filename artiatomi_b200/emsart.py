@@ -122,6 +122,22 @@ def mag_aniso_matrix(amount: float, angle_deg: float, dim_x: float, dim_y: float
     return out
 
 
+def autotune(enable: int = 1) -> None:
+    """Launch-shape autotuning of the reconstructor's fast kernels: 1 measure
+    (default), 0 cached or default shapes only, -1 clear the cache, k >= 2
+    every tuned kernel takes its candidate k - 2 (for tests)."""
+    check(lib.esb_autotune(int(enable)))
+
+
+def autotune_report() -> str:
+    """The cached launch-shape choices, one line per problem shape."""
+    need = C.c_size_t(0)
+    check(lib.esb_autotune_report(None, 0, C.byref(need)))
+    buf = C.create_string_buffer(need.value)
+    check(lib.esb_autotune_report(buf, need.value, None))
+    return buf.value.decode()
+
+
 def rotation_matrix(phi: float, psi: float, theta: float) -> np.ndarray:
     """RotKernel::computeRotMat: 3 x 3 rotation of the motive list's Euler
     angles (degrees, ZXZ)."""

@@ -343,7 +343,8 @@ def run_esb(args):
                            "oversampling": params["os"], "sirt_count": sirt, "ctf": params["ctf"],
                            "ctf_slab_nm": 30.0, "voxel_storage": "f32", "kernels": args.variant,
                            "l2": f"inputs larger than L2 (volume {wl.voxels * 4 / 2**20:.0f} MiB)",
-                           "parallelism": f"replicas x{ws}"},
+                           "parallelism": f"replicas x{ws}",
+                           "launch_shapes": E.autotune_report().strip().splitlines()},
                 "e2e": {"value": e2e_value, "unit": UNIT,
                         "h2d_bytes_per_step": int(wl.projections.numel() * 4),
                         "d2h_bytes_per_step": int(vol.numel() * 4)},

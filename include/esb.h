@@ -104,6 +104,22 @@ int esb_version(void);
  * reference: a diagnostic for launch-count claims. */
 unsigned long long esb_kernel_launches(void);
 
+/* Autotuning of launch shapes (no counterpart in the reference). A
+ * reconstructor picks, per GPU and problem shape, the block shape of the fast
+ * projector and of the single-axis back-projector the first time it launches
+ * them outside stream capture (CUDA events; one warm-up and two timed trial
+ * launches per candidate; trials never write the caller's volume), and the
+ * choice is cached for the process. Results do not depend on the shape.
+ * enable: 1 measure (default), 0 use cached or default shapes only, -1 clear
+ * the cache (measuring stays as it was), k >= 2 make every tuned kernel take
+ * its candidate k - 2 (the last one where it has fewer; for tests: results
+ * must not change); 0 or 1 end that. */
+int esb_autotune(int enable);
+/* The cached choices as text, one line per problem shape, into buf
+ * (NUL-terminated, truncated to len; buf may be NULL with len 0); *needed
+ * (may be NULL) = the bytes the whole text takes, NUL included. */
+int esb_autotune_report(char* buf, size_t len, size_t* needed);
+
 /* ---------------------------------------------------------------- geometry
  * Host functions; no device work. */
 

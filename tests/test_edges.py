@@ -258,3 +258,44 @@ def test_fast_projection_of_a_volume_above_2_32_voxels():
         assert rel_l2(outs[0], outs[1]) <= 1e-3, (i, rel_l2(outs[0], outs[1]))
     del big
     torch.cuda.empty_cache()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ctf", [False, True])
+def test_autotuned_launch_shapes_do_not_change_results(ctf):
+    """The reconstructor's launch-shape autotuner: every candidate shape of
+    the fast projector and the single-axis back-projector gives the same
+    volume bit for bit, the tuned run as well, and the choices are cached
+    per problem shape."""
+    import artiatomi_b200 as E
+    from tests.test_parity_recon import _ctf_cfg, _projections
+
+    case = small_case(dims=(48, 40, 20), n_proj=5, W=56, H=48, shift=1.0, psi=0.3)
+    W, H, n = case["W"], case["H"], len(case["tilt"])
+    projs = cuda(_projections(case))
+    il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, case["tilt"])
+    defocus = np.tile(np.array([3000.0, 3080.0, 25.0], np.float32), n) if ctf else None
+    cfgd = dict(_ctf_cfg(max(W, H)), lambda_=0.5, oversampling=2) if ctf else dict(lambda_=0.5, oversampling=2)
+
+    def run():
+        rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **cfgd), case["pg"], case["tilt"],
+                              defocus)
+        v = cuda(np.zeros(case["vol"].shape, np.float32))
+        rec.sart(case["vg"], v, projs, il, iterations=1, sirt_count=2)
+        return host(v)
+
+    try:
+        vols = []
+        for k in range(5):  # candidate k of every tuned kernel
+            E.autotune(2 + k)
+            vols.append(run())
+        E.autotune(-1)
+        E.autotune(1)
+        vols.append(run())
+        report = E.autotune_report()
+    finally:
+        E.autotune(1)
+    assert np.abs(vols[0]).max() > 0
+    for v in vols[1:]:
+        np.testing.assert_array_equal(v, vols[0])
+    assert "bp_axis" in report and ("fp_slicer_fused" if ctf else "fp_march") in report, report
