@@ -1468,12 +1468,12 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
   if (batched && cf.variant == ESB_VARIANT_FAST && n_particles > 0 && proj_count > 0) {
     std::vector<KConst> consts((size_t)n_particles * proj_count);
     std::vector<unsigned char> act((size_t)n_particles * proj_count);
-    for (int p = 0; p < n_particles; ++p)
-      for (int ii = 0; ii < proj_count; ++ii) {
-        const size_t pair = (size_t)p * np + index_list[ii];
-        consts[(size_t)p * proj_count + ii] = rec_const(r, pair_geoms[pair], sub_geoms[p], 1);
-        act[(size_t)p * proj_count + ii] = active ? (active[pair] != 0) : 1;
-      }
+    host_parallel_for((long)n_particles * proj_count, [&](long i) {
+      const int p = (int)(i / proj_count), ii = (int)(i % proj_count);
+      const size_t pair = (size_t)p * np + index_list[ii];
+      consts[i] = rec_const(r, pair_geoms[pair], sub_geoms[p], 1);
+      act[i] = active ? (active[pair] != 0) : 1;
+    });
     if (subvol_batchable(n_particles, boxes, consts.data(), proj_count)) {
       ESB_CK(subvol_batch_build(r->batch, n_particles, boxes, consts.data(), act.data(), proj_count, cf.oversampling,
                                 r->stream), "esb_subvolume_wbp");

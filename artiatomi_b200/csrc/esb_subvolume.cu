@@ -164,23 +164,36 @@ cudaError_t subvol_batch_build(SubvolBatch& b, int n_particles, float* const* bo
   b.off_parts = align256(work.size() * sizeof(SubvolWork));
   b.off_pairs = b.off_parts + align256(parts.size() * sizeof(SubvolParticle));
   const size_t bytes = b.off_pairs + n_pairs * sizeof(PairConst);
-  b.host.resize(bytes);
-  memcpy(b.host.data(), work.data(), work.size() * sizeof(SubvolWork));
-  memcpy(b.host.data() + b.off_parts, parts.data(), parts.size() * sizeof(SubvolParticle));
-  PairConst* pc = (PairConst*)(b.host.data() + b.off_pairs);
-  b.all_axis = 1;
-  for (size_t i = 0; i < n_pairs; ++i) {
-    pc[i].k = consts[i];
-    pc[i].g = make_geom(consts[i], os);
-    pc[i].axis = axis_eligible(consts[i], pc[i].g) ? 1 : 0;
-    if (pc[i].axis)
-      pc[i].a = make_axis_geom(consts[i], pc[i].g, os);
-    else
-      b.all_axis = 0;
-    pc[i].active = !active || active[i];
+  cudaError_t e;
+  // the staging buffer is pinned (the copy runs asynchronously): wait for
+  // the previous call's copy before writing it again
+  if (b.copied && (e = cudaEventSynchronize(b.copied)) != cudaSuccess) return e;
+  if (!b.copied && (e = cudaEventCreateWithFlags(&b.copied, cudaEventDisableTiming)) != cudaSuccess) return e;
+  if (bytes > b.host_cap) {
+    cudaFreeHost(b.host);
+    b.host = nullptr;
+    b.host_cap = 0;
+    if ((e = cudaHostAlloc((void**)&b.host, bytes, cudaHostAllocDefault)) != cudaSuccess) return e;
+    b.host_cap = bytes;
   }
+  memcpy(b.host, work.data(), work.size() * sizeof(SubvolWork));
+  memcpy(b.host + b.off_parts, parts.data(), parts.size() * sizeof(SubvolParticle));
+  PairConst* pc = (PairConst*)(b.host + b.off_pairs);
+  // per-pair constants on the host cores (the tables of 2000 particles x 61
+  // tilts are 1.2e5 pairs)
+  host_parallel_for((long)n_pairs, [&](long i) {
+    PairConst& q = pc[i];
+    q.k = consts[i];
+    q.g = make_geom(consts[i], os);
+    q.axis = axis_eligible(consts[i], q.g) ? 1 : 0;
+    if (q.axis) q.a = make_axis_geom(consts[i], q.g, os);
+    q.active = !active || active[i];
+  });
+  b.all_axis = 1;
+  for (size_t i = 0; i < n_pairs; ++i)
+    if (!pc[i].axis) b.all_axis = 0;
   if (bytes > b.cap) {
-    cudaError_t e = cudaStreamSynchronize(st);  // the old tables may be in use
+    e = cudaStreamSynchronize(st);  // the old tables may be in use
     if (e != cudaSuccess) return e;
     cudaFree(b.dev);
     b.dev = nullptr;
@@ -190,7 +203,8 @@ cudaError_t subvol_batch_build(SubvolBatch& b, int n_particles, float* const* bo
   }
   b.n_work = (int)work.size();
   b.n_list = n_list;
-  return cudaMemcpyAsync(b.dev, b.host.data(), bytes, cudaMemcpyHostToDevice, st);
+  if ((e = cudaMemcpyAsync(b.dev, b.host, bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  return cudaEventRecord(b.copied, st);
 }
 
 cudaError_t subvol_batch_launch(const SubvolBatch& b, int t0, int nt, const float* imgs, size_t img_stride,
@@ -221,8 +235,12 @@ void subvol_batch_free(SubvolBatch& b) {
   cudaFree(b.dev);
   b.dev = nullptr;
   b.cap = 0;
-  b.host.clear();
-  b.host.shrink_to_fit();
+  if (b.copied) cudaEventSynchronize(b.copied);
+  cudaFreeHost(b.host);
+  b.host = nullptr;
+  b.host_cap = 0;
+  if (b.copied) cudaEventDestroy(b.copied);
+  b.copied = nullptr;
 }
 
 }  // namespace esb

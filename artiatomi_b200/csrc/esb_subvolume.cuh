@@ -3,11 +3,33 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "esb_device.cuh"
 
 namespace esb {
+
+// f(i) for i in [0, n) on the host cores (chunks of consecutive i per
+// thread; serial below `serial_below` items).
+template <class F>
+void host_parallel_for(long n, F f, long serial_below = 4096) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const long nt = std::min<long>(std::max(1u, std::min(hw, 32u)), (n + serial_below - 1) / std::max(serial_below, 1L));
+  if (nt <= 1) {
+    for (long i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const long chunk = (n + nt - 1) / nt;
+  for (long t = 0; t < nt; ++t)
+    pool.emplace_back([=, &f]() {
+      const long e = std::min(n, (t + 1) * chunk);
+      for (long i = t * chunk; i < e; ++i) f(i);
+    });
+  for (auto& th : pool) th.join();
+}
 
 // Device tables of one batched call: the work list (blocks of 128 voxel
 // quads of one particle), the particles' boxes and the kernel constants of
@@ -16,7 +38,9 @@ namespace esb {
 struct SubvolBatch {
   void* dev = nullptr;
   size_t cap = 0;
-  std::vector<unsigned char> host;  // staging copy of the tables
+  unsigned char* host = nullptr;  // pinned staging copy of the tables
+  size_t host_cap = 0;
+  cudaEvent_t copied = nullptr;   // the last copy of the staging buffer to the device
   size_t off_parts = 0, off_pairs = 0;
   int n_work = 0;
   int n_list = 0;
