@@ -151,7 +151,7 @@ def test_projection_loss_grad_roi_matches_full_image():
         np.testing.assert_allclose(host(o8)[6:], [(pd * pd).sum(), (pd * meas).sum()], rtol=1e-6)
 
 
-def _refine_dataset(tmp_path):
+def _refine_dataset(tmp_path, bad=None):
     """Background phantom with the particle cubes zeroed, plus three rotated
     references projected with known extra shifts; files as EmSart and
     EmSartRefine read them."""
@@ -197,6 +197,8 @@ def _refine_dataset(tmp_path):
     F.write_mrc(str(tmp_path / "ts.mrc"), raw, 0.5)
     items = np.zeros((1, n, 10), np.float32)
     items[0, :, 0], items[0, :, 1:3], items[0, :, 8], items[0, :, 9] = tilt, 10.0, 1.0, psi
+    if bad is not None:
+        items[0, bad, 1:3] = -1.0  # reference marker not clicked: projection unusable
     F.write_markers(str(tmp_path / "markers.em"), items)
     F.write_em(str(tmp_path / "vol.em"), -back)  # EmSart writes the volume negated
     F.write_em(str(tmp_path / "ref.em"), ref)
@@ -249,7 +251,8 @@ MultiPeakDetection = false
 
 
 @pytest.mark.gpu
-def test_refine_recovers_extra_shifts(tmp_path):
+@pytest.mark.parametrize("bad", [None, 2])
+def test_refine_recovers_extra_shifts(tmp_path, bad):
     """Every particle's per-tilt extra shift comes back within 0.05 px (the
     data's rays start from the shifted detector, the fitted model translates
     the unshifted rays' samples: their sample depths differ by up to a
@@ -259,10 +262,14 @@ def test_refine_recovers_extra_shifts(tmp_path):
     from artiatomi_b200.config import EmSartConfig
     from artiatomi_b200.refine import refine_shifts
 
-    es = _refine_dataset(tmp_path)
+    es = _refine_dataset(tmp_path, bad)
     cfg = EmSartConfig.from_file(str(tmp_path / "refine.cfg"), refine=True)
     got = refine_shifts(cfg)
     assert got.shape == es.shape
+    if bad is not None:  # an unusable projection keeps zero shifts
+        assert np.all(got[bad] == 0.0)
+        es = es.copy()
+        es[bad] = 0.0
     err = np.abs(got - es).max()
     assert err <= 5e-2, (err, got, es)
     np.testing.assert_array_equal(F.read_shift_file(cfg.ShiftOutputFile), got)
