@@ -662,8 +662,9 @@ int esb_rec_reset_projections(esb_reconstructor* r) {
 // is timed with CUDA events on the reconstructor's stream (one warm-up
 // launch, two timed ones) and the fastest is cached for the process.
 // Projector candidates read the real volume and write scratch images;
-// back-projection candidates run on a 16-plane scratch slab from the middle
-// of the volume, so the caller's volume is never written by a trial. During
+// back-projection candidates run on a scratch slab of up to 32 planes from
+// the middle of the volume, so the caller's volume is never written by a
+// trial; the scratch is released once the trials are done. During
 // capture, or when tuning is off, the cached or the default shape is taken.
 namespace {
 struct TuneKey {
@@ -747,6 +748,10 @@ static int rec_tuned(esb_reconstructor* r, const TuneKey& key, int n, int def, R
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  // the trials are done (synchronised above): release their scratch
+  cudaFree(r->tune_scratch);
+  r->tune_scratch = nullptr;
+  r->tune_cap = 0;
   std::lock_guard<std::mutex> lock(g_tune_mu);
   g_tune[key] = best;
   return best;
@@ -819,13 +824,13 @@ static int rec_march_nw(esb_reconstructor* r, const KConst& c, const void* vol, 
 }
 
 // Block shape of the single-axis back-projection for this problem; trials on
-// a scratch slab of up to 16 planes from the middle of the volume.
+// a scratch slab of up to 32 planes from the middle of the volume.
 static BpShape rec_bp_shape(esb_reconstructor* r, const KConst& c, int vt, const float* imgs, size_t img_stride,
                             const SlabTable& T, int linear, const float* up, size_t up_stride) {
   const int W = r->cfg.proj_x, H = r->cfg.proj_y, os = r->cfg.oversampling;
   BpShape s{kBpShapes[0][0], kBpShapes[0][1], 0, 0};
   if (!bp_uses_axis(c, os)) return s;
-  const int nz = (int)c.dim.z, planes = std::min(nz, 16);
+  const int nz = (int)c.dim.z, planes = std::min(nz, 32);
   const size_t plane = (size_t)c.dim.x * (size_t)c.dim.y * (vt == ESB_VOXEL_F32 ? 4 : 2);
   const int i = rec_tuned(r, tune_key(r, 2, vt, c, T.count > 0), kNBpShapes, 0, [&](int k) {
     void* slab = rec_tune_scratch(r, plane * planes);

@@ -189,7 +189,10 @@ __device__ float layer_sum_xz(const Cell<VT>& C, float qx, float b, int iy, floa
   float enn = ey(on + omn), efn = ey(of + omn);
   const float Mt = (float)(J - j0);
   float fm0 = 0.0f, acc = 0.0f;
-#pragma unroll 1
+  // two layers per iteration give the scheduler independent loads; the
+  // 64-bit-offset instances stay at one (registers)
+  constexpr int kUnroll = sizeof(Off) == 4 ? 2 : 1;
+#pragma unroll kUnroll
   for (int guard = 0; guard < 1 << 20; ++guard) {
     // samples [fm0, fmA) lie in cell (n, m), [fmA, fmL) in cell (n + 1, m)
     const float fmL = nMs >= Mt ? Mt : ceilf(nMs);
