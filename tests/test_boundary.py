@@ -72,3 +72,24 @@ def test_kernel_launch_counter_counts_launches():
     E.forward_project(c, vol, proj, dist)
     E.forward_project(c, vol, proj, dist, fast=True)
     assert E.kernel_launches() - n0 == 2
+
+
+def test_autotune_switch_and_report():
+    """The launch-shape autotuner's C ABI without a GPU: the switch values,
+    the refusal of others, and the report of an empty cache."""
+    import ctypes as C
+
+    import artiatomi_b200 as E
+    from artiatomi_b200 import _lib as L
+
+    try:
+        for v in (0, 1, -1, 2, 5, 1):
+            E.autotune(v)
+        with pytest.raises(L.EsbError):
+            E.autotune(-2)
+        E.autotune(-1)
+        assert E.autotune_report() == ""
+        need = C.c_size_t(0)
+        assert L.lib.esb_autotune_report(None, 0, C.byref(need)) == 0 and need.value == 1
+    finally:
+        E.autotune(1)
