@@ -34,6 +34,7 @@ UNITS = [
     ("esb_subvolume.cu", []),
     ("esb_adjoint.cu", []),
     ("esb_refine.cu", []),
+    ("esb_cc.cu", ["--fmad=false"]),
     ("esb_image.cu", ["--fmad=false"]),
     ("esb_api.cu", []),
     ("esb_noalloc.cu", []),

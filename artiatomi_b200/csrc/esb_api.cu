@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <string>
@@ -66,6 +68,12 @@ cudaError_t launch_loss_grad(const KConst& c, const void* vol, int vt, const flo
                              float sy, float* grad, float* proj_out, double* out, int w, int h, cudaStream_t st,
                              const int* roi = nullptr);
 cudaError_t launch_rotate_volume(const float* in, float* out, int size, const float rot[9], cudaStream_t st);
+cudaError_t launch_cc_center(float* sq, long n, double* sums, cudaStream_t st);
+cudaError_t launch_cc_conj_mul(float* a, const float* b, long n_complex, cudaStream_t st);
+cudaError_t launch_cc_map(const float* cc, int n, int s, const double* sums, float* map, cudaStream_t st);
+cudaError_t launch_cc_finish(float* cc, int n, int s, const double* sums, unsigned long long* key, cudaStream_t st);
+cudaError_t launch_cc_peaks(const float* img, float* out, int n, int s, const unsigned long long* key,
+                            unsigned long long* key2, cudaStream_t st);
 cudaError_t launch_convert_input(const void* in, int type, long n, float* out, cudaStream_t st);
 cudaError_t launch_window_stats(const float* img, size_t pitchE, int x0, int y0, int w, int h, double* out,
                                 cudaStream_t st);
@@ -457,6 +465,11 @@ struct esb_reconstructor {
   double* prep_stats = nullptr;
   cufftHandle prep_r2c = 0, prep_c2r = 0;
   bool prep_plans = false;
+  // cross-correlation displacement: two squares, two spectra, the sums of
+  // both squares (4 doubles) and two arg-max keys
+  float* cc_sq = nullptr;
+  float* cc_spec = nullptr;
+  void* cc_red = nullptr;
 };
 
 // Brackets a phase of launches with events when timing is enabled.
@@ -530,6 +543,11 @@ static void rec_free(esb_reconstructor* r) {
     cufftDestroy(r->prep_c2r);
     r->prep_plans = false;
   }
+  cudaFree(r->cc_sq);
+  cudaFree(r->cc_spec);
+  cudaFree(r->cc_red);
+  r->cc_sq = r->cc_spec = nullptr;
+  r->cc_red = nullptr;
   cudaFree(r->spec_batch);
   cudaFree(r->sq_batch);
   r->spec_batch = r->sq_batch = nullptr;
@@ -1387,6 +1405,83 @@ int esb_prepare_projection(esb_reconstructor* r, const esb_prepare_config* pc, c
   if (mean_out) *mean_out = meanValue;
   if (std_out) *std_out = stdValue;
   if (bad_out) *bad_out = bad;
+  return ok();
+}
+
+int esb_rec_cc_displacement(esb_reconstructor* r, const float* residual, const float* model, int max_shift,
+                            int multi_peak, float* shift_xy, float* cc_value, float* cc_map, float* cc_map_multi) {
+  if (!r || !residual || !model || !shift_xy)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_cc_displacement: NULL argument");
+  const int W = r->cfg.proj_x, H = r->cfg.proj_y, N = r->N;
+  if (max_shift < 1 || 2 * max_shift > N)
+    return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_cc_displacement: max_shift must be in [1, N/2] for the N x N square");
+  if (N > 65535) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_cc_displacement: square larger than 65535");
+  const long nsq = (long)N * N, nspec = (long)(N / 2 + 1) * N;
+  cudaStream_t st = r->stream;
+  if (!r->cc_sq) ESB_CK(cudaMalloc(&r->cc_sq, 2 * nsq * sizeof(float)), "esb_rec_cc_displacement");
+  if (!r->cc_spec) ESB_CK(cudaMalloc(&r->cc_spec, 2 * nspec * 2 * sizeof(float)), "esb_rec_cc_displacement");
+  if (!r->cc_red) ESB_CK(cudaMalloc(&r->cc_red, 4 * sizeof(double) + 2 * sizeof(unsigned long long)),
+                         "esb_rec_cc_displacement");
+  // the N x N plans: the CTF configuration's, else the preparation's
+  cufftHandle r2c = r->r2c, c2r = r->c2r;
+  if (!r->plans) {
+    if (!r->prep_plans) {
+      ESB_FFT(cufftPlan2d(&r->prep_r2c, N, N, CUFFT_R2C), "esb_rec_cc_displacement");
+      ESB_FFT(cufftPlan2d(&r->prep_c2r, N, N, CUFFT_C2R), "esb_rec_cc_displacement");
+      r->prep_plans = true;
+    }
+    r2c = r->prep_r2c;
+    c2r = r->prep_c2r;
+  }
+  ESB_FFT(cufftSetStream(r2c, st), "esb_rec_cc_displacement");
+  ESB_FFT(cufftSetStream(c2r, st), "esb_rec_cc_displacement");
+  float *sqA = r->cc_sq, *sqB = r->cc_sq + nsq;
+  float *specA = r->cc_spec, *specB = r->cc_spec + 2 * nspec;
+  double* sums = (double*)r->cc_red;  // [sum A, sum of squares A, sum B, sum of squares B]
+  unsigned long long* keys = (unsigned long long*)(sums + 4);
+  ESB_CK(cudaMemsetAsync(r->cc_red, 0, 4 * sizeof(double) + 2 * sizeof(unsigned long long), st),
+         "esb_rec_cc_displacement");
+  // Reconstructor.cpp:1769-1815: mirror-padded squares centred on their
+  // means, sums of squares, spectra
+  ESB_CK(launch_make_square(W, H, W, residual, N, sqA, r->borderX, r->borderY, 0, 0, st), "esb_rec_cc_displacement");
+  ESB_CK(launch_cc_center(sqA, nsq, sums, st), "esb_rec_cc_displacement");
+  ESB_FFT(cufftExecR2C(r2c, (cufftReal*)sqA, (cufftComplex*)specA), "esb_rec_cc_displacement R2C");
+  ESB_CK(launch_make_square(W, H, W, model, N, sqB, r->borderX, r->borderY, 0, 0, st), "esb_rec_cc_displacement");
+  ESB_CK(launch_cc_center(sqB, nsq, sums + 2, st), "esb_rec_cc_displacement");
+  ESB_FFT(cufftExecR2C(r2c, (cufftReal*)sqB, (cufftComplex*)specB), "esb_rec_cc_displacement R2C");
+  // :1817-1866: correlation, normalisation, map, maxShift mask, arg-max
+  ESB_CK(launch_cc_conj_mul(specA, specB, nspec, st), "esb_rec_cc_displacement");
+  ESB_FFT(cufftExecC2R(c2r, (cufftComplex*)specA, (cufftReal*)sqA), "esb_rec_cc_displacement C2R");
+  if (cc_map) ESB_CK(launch_cc_map(sqA, N, max_shift, sums, cc_map, st), "esb_rec_cc_displacement");
+  ESB_CK(launch_cc_finish(sqA, N, max_shift, sums, keys, st), "esb_rec_cc_displacement");
+  // :1886-1932: the peak nearest the origin among those >= 0.9 x maximum
+  if (multi_peak) {
+    ESB_CK(launch_cc_peaks(sqA, sqB, N, max_shift, keys, keys + 1, st), "esb_rec_cc_displacement");
+    if (cc_map_multi) ESB_CK(launch_cc_map(sqB, N, max_shift, nullptr, cc_map_multi, st), "esb_rec_cc_displacement");
+  }
+  unsigned long long k[2];
+  ESB_CK(cudaMemcpyAsync(k, keys, sizeof(k), cudaMemcpyDeviceToHost, st), "esb_rec_cc_displacement");
+  ESB_CK(cudaStreamSynchronize(st), "esb_rec_cc_displacement");
+  // key -> value and raster index (the order-preserving map of esb_cc.cu)
+  auto value = [](unsigned long long key) {
+    if (key == 0ull) return std::numeric_limits<float>::quiet_NaN();
+    uint32_t u = (uint32_t)(key >> 32);
+    u = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
+    float v;
+    std::memcpy(&v, &u, sizeof(v));
+    return v;
+  };
+  const float maxVal = value(k[0]);
+  const unsigned long long kk = multi_peak ? k[1] : k[0];
+  const long idx = kk ? (long)(0xFFFFFFFFu - (uint32_t)(kk & 0xFFFFFFFFull)) : 0;
+  float sx = (float)(idx % N), sy = (float)(idx / N);
+  // :1941-1957: signed shifts; no positive correlation: no shift found
+  if (sx > (float)(N / 2)) sx -= (float)N;
+  if (sy > (float)(N / 2)) sy -= (float)N;
+  if (!(maxVal > 0.0f)) sx = sy = -1000.0f;
+  shift_xy[0] = sx;
+  shift_xy[1] = sy;
+  if (cc_value) *cc_value = maxVal;
   return ok();
 }
 

@@ -484,6 +484,19 @@ class Reconstructor:
                                          C.byref(b)))
         return m.value, s.value, b.value
 
+    def cc_displacement(self, residual, model, max_shift: int, multi_peak: bool = False, cc_map=None,
+                        cc_map_multi=None):
+        """GetDisplacement (Reconstructor.cpp:1746-1960): the integer shift
+        (x, y) at the maximum of the normalised cross-correlation of two
+        H x W device images, and that maximum. cc_map / cc_map_multi:
+        optional (4 max_shift)^2 device tensors for the correlation's centre
+        and the multi-peak map."""
+        sh = np.zeros(2, np.float32)
+        v = C.c_float()
+        check(lib.esb_rec_cc_displacement(self._h, fptr(residual), fptr(model), int(max_shift), int(multi_peak),
+                                          fptr(sh), C.byref(v), fptr(cc_map), fptr(cc_map_multi)))
+        return (float(sh[0]), float(sh[1])), v.value
+
     def forward_projection(self, vg, vol, index: int, volume_is_empty: bool = False):
         check(lib.esb_rec_forward_projection(self._h, C.byref(vg), fptr(vol), _voxel_type_of(vol), index,
                                              int(volume_is_empty)))

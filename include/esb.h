@@ -427,6 +427,27 @@ typedef struct {
 int esb_prepare_projection(esb_reconstructor* rec, const esb_prepare_config* pc, const void* in, float* out,
                            float* mean, float* std_dev, int* bad_pixels);
 
+/* Reconstructor::GetDisplacement (Reconstructor.cpp:1746-1960), EmSartRefine's
+ * shift measurement: residual (the compare image of the reconstruction
+ * without the particles) and model (the particles' projection), device,
+ * W x H dense, are mirror-padded to the N x N square, centred on their
+ * means and cross-correlated (conjMul, wbpWeighting.cu:244-262); the
+ * correlation is divided by N^2 sqrt(SumA SumB), values farther than
+ * max_shift from the origin are zeroed (maxShift, :266-293) and the
+ * arg-max gives the integer shift (x, y), folded to (-N/2, N/2]. With
+ * multi_peak the local maxima of at least 0.9 x the maximum (findPeak,
+ * :331-386) are weighted by 1 / (distance + 1e-4) (maxShiftWeighted,
+ * :296-327) and that map's arg-max gives the shift. A maximum <= 0 gives
+ * (-1000, -1000), as in the reference, and so does a correlation that is
+ * NaN everywhere. Ties go to the first pixel in raster order.
+ * shift_xy (host, 2 floats); cc_value (host, may be NULL): the maximum of
+ * the normalised correlation; cc_map, cc_map_multi (device, may be NULL):
+ * the (4 max_shift)^2 fft-shifted centre of the correlation and of the
+ * multi-peak map (the reference's ccMap and ccMapMulti). 1 <= max_shift
+ * <= N/2. Synchronises the reconstructor's stream. */
+int esb_rec_cc_displacement(esb_reconstructor* rec, const float* residual, const float* model, int max_shift,
+                            int multi_peak, float* shift_xy, float* cc_value, float* cc_map, float* cc_map_multi);
+
 /* The SART driver loop of EmSart.cpp:579-675 for one GPU: iterations x
  * ordered subsets of sirt_count projections x {FP, compare} then {BP}.
  * projections: device, n_proj images of W x H (already prepared);

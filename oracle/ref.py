@@ -30,6 +30,9 @@ _SIGS = {
     "ref_fourier_filter": [P, I, F, F, F, F],
     "ref_dose_weighting": [P, I, F, F],
     "ref_rot3d": [P, P, I, P, I, I],
+    "ref_conj_mul": [P, P, I],
+    "ref_max_shift": [P, I, I, I],
+    "ref_find_peak": [P, P, I, F],
 }
 
 _lib = None
@@ -98,3 +101,26 @@ def fourier_filter(spec, lp, hp, lps, hps):
 
 def dose_weighting(spec, dose, ps):
     lib().ref_dose_weighting(addr(spec), spec.shape[0], dose, ps)
+
+
+def conj_mul(a, b):
+    """conjMul on complex64 half spectra (N x N/2+1): returns conj(a) * b."""
+    out = np.ascontiguousarray(a, np.complex64).copy()
+    bb = np.ascontiguousarray(b, np.complex64)
+    lib().ref_conj_mul(addr(out), addr(bb), out.shape[0])
+    return out
+
+
+def max_shift(img, s, weighted=False):
+    """maxShift / maxShiftWeighted on an N x N float32 image (a copy)."""
+    out = f32(img).copy()
+    lib().ref_max_shift(addr(out), out.shape[0], int(s), int(weighted))
+    return out
+
+
+def find_peak(img, threshold):
+    """findPeak: uint8 mask, 0 at the local maxima >= threshold, 1 elsewhere."""
+    im = f32(img)
+    mask = np.full(im.shape, 7, np.uint8)
+    lib().ref_find_peak(addr(im), addr(mask), im.shape[0], float(threshold))
+    return mask

@@ -51,3 +51,30 @@ extern "C" int ref_rot3d(const float* in, float* out, int size, const float* rot
            [&]() { ref_wbp::rot3d(size, r0, r1, r2, out); });
   return 0;
 }
+
+// Kernels of GetDisplacement (Reconstructor.cpp:1746-1960), launched as
+// ConjKernel, MaxShiftKernel, MaxShiftWeightedKernel and FindPeakKernel do
+// (16 x 16 blocks; Reconstructor.cpp:252-266): conjMul over the N/2+1 x N
+// half spectra, the others over the N x N correlation.
+extern "C" int ref_conj_mul(float* a, const float* b, int n) {
+  const size_t stride = (size_t)(n / 2 + 1) * sizeof(float2);
+  esb_grid(dim3((n / 2 + 1 + 15) / 16, (n + 15) / 16), dim3(16, 16), 1,
+           [&]() { ref_wbp::conjMul((float2*)a, (float2*)b, stride, n); });
+  return 0;
+}
+
+extern "C" int ref_max_shift(float* img, int n, int max_shift, int weighted) {
+  const size_t stride = (size_t)n * sizeof(float);
+  esb_grid(dim3((n + 15) / 16, (n + 15) / 16), dim3(16, 16), 1, [&]() {
+    if (weighted) ref_wbp::maxShiftWeighted(img, stride, n, max_shift);
+    else ref_wbp::maxShift(img, stride, n, max_shift);
+  });
+  return 0;
+}
+
+extern "C" int ref_find_peak(float* img, unsigned char* mask, int n, float threshold) {
+  const size_t stride = (size_t)n * sizeof(float);
+  esb_grid(dim3((n + 15) / 16, (n + 15) / 16), dim3(16, 16), 1,
+           [&]() { ref_wbp::findPeak(img, stride, (char*)mask, (size_t)n, n, threshold); });
+  return 0;
+}

@@ -201,7 +201,7 @@ def _refine_dataset(tmp_path, bad=None):
         items[0, bad, 1:3] = -1.0  # reference marker not clicked: projection unusable
     F.write_markers(str(tmp_path / "markers.em"), items)
     F.write_em(str(tmp_path / "vol.em"), -back)  # EmSart writes the volume negated
-    F.write_em(str(tmp_path / "ref.em"), ref)
+    F.write_em(str(tmp_path / "ref.em"), -ref)  # an average of negated sub-volumes
     motl = np.zeros((3, 20), np.float32)
     motl[:, 3] = np.arange(1, 4)
     motl[:, 7:10] = pos
@@ -264,7 +264,7 @@ def test_refine_recovers_extra_shifts(tmp_path, bad):
 
     es = _refine_dataset(tmp_path, bad)
     cfg = EmSartConfig.from_file(str(tmp_path / "refine.cfg"), refine=True)
-    got = refine_shifts(cfg)
+    got = refine_shifts(cfg, method="lsq")
     assert got.shape == es.shape
     if bad is not None:  # an unusable projection keeps zero shifts
         assert np.all(got[bad] == 0.0)
@@ -273,3 +273,42 @@ def test_refine_recovers_extra_shifts(tmp_path, bad):
     err = np.abs(got - es).max()
     assert err <= 5e-2, (err, got, es)
     np.testing.assert_array_equal(F.read_shift_file(cfg.ShiftOutputFile), got)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("multi", [False, True])
+def test_refine_cc_recovers_integer_shifts(tmp_path, multi):
+    """The reference's measurement (cross-correlation peak): every shift is
+    an integer within 0.6 px of the true extra shift (0.5 from rounding),
+    the ShiftFile holds what EmSARTSubVolumes reads, and with CCMapFileName
+    set one (4 MaxShift)^2 map per particle is written per projection."""
+    from artiatomi_b200 import fileio as F
+    from artiatomi_b200.config import EmSartConfig
+    from artiatomi_b200.refine import refine_shifts
+
+    es = _refine_dataset(tmp_path)
+    cfg = EmSartConfig.from_file(str(tmp_path / "refine.cfg"), refine=True)
+    cfg.MultiPeakDetection = multi
+    cfg.CCMapFileName = str(tmp_path / "ccmap_")
+    got = refine_shifts(cfg)
+    assert got.shape == es.shape
+    np.testing.assert_array_equal(got, np.round(got))
+    err = np.abs(got - es)
+    assert err.max() <= 0.6 and err.mean() <= 0.35, (err, got, es)
+    np.testing.assert_array_equal(F.read_shift_file(cfg.ShiftOutputFile), got)
+    S = cfg.MaxShift
+    for i in range(es.shape[0]):
+        maps, _ = F.read_em(str(tmp_path / f"ccmap_{i}.em"))
+        assert maps.shape == (3, 4 * S, 4 * S)
+        # the centre of each map is the zero shift; the maximum sits at the
+        # measured shift (the unmasked map holds no larger value inside MaxShift)
+        for p in range(3):
+            c = 2 * S
+            m = maps[p].copy()
+            yy, xx = np.mgrid[0:4 * S, 0:4 * S]
+            m[(xx - c) ** 2 + (yy - c) ** 2 > S * S] = -np.inf
+            y, x = np.unravel_index(np.argmax(m), m.shape)
+            if not multi:
+                assert (x - c, y - c) == (-got[i, p, 0], -got[i, p, 1])
+        if multi:
+            assert F.read_em(str(tmp_path / f"ccmap_Multi_{i}.em"))[0].shape == (3, 4 * S, 4 * S)
