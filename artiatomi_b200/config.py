@@ -117,6 +117,9 @@ class EmSartConfig:
     SpeedUpDistance: int = 0
     MultiPeakDetection: bool = False
     CCMapFileName: str = ""
+    SupportingReferences: list = field(default_factory=list)
+    SupportingMotiveLists: list = field(default_factory=list)
+    MaxDistanceSupport: float = 0.0
 
     @classmethod
     def from_text(cls, text: str, subvolumes: bool = False, refine: bool = False) -> "EmSartConfig":
@@ -225,6 +228,15 @@ class EmSartConfig:
             c.ScaleMotivelistShift = float(req("ScaleMotivelistShift"))
             c.ScaleMotivelistPosition = float(req("ScaleMotivelistPosition"))
             c.MultiPeakDetection = _bool(req("MultiPeakDetection"))
+            # ';'-separated lists; items of 3 characters or fewer are dropped
+            # (utils/Config.cpp:449-475)
+            refs = opt("SupportingReferences", "")
+            if len(refs) > 3:
+                c.SupportingReferences = [it for it in refs.split(";") if len(it) > 3]
+                lists = req("SupportingMotiveLists")
+                if len(lists) > 3:
+                    c.SupportingMotiveLists = [it for it in lists.split(";") if len(it) > 3]
+                c.MaxDistanceSupport = float(req("MaxDistanceSupport"))
         return c
 
     @classmethod

@@ -94,20 +94,91 @@ def _fit_shift(c_sub, ref, target, roi, iterations, max_shift, out):
     return s
 
 
-def _cc_shift(R, vg, i, c_full, vol, c_sub, rot, roi, bufs, max_shift, multi, maps):
+def _distance(a, b):
+    """MotiveList::GetDistance (MotiveList.cpp:121-130): float distance of two
+    particles' coordinates."""
+    d = (a[7:10] - b[7:10]).astype(np.float32)
+    return np.float32(np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])))
+
+
+def global_index(motl, i):
+    """MotiveList::GetGlobalIdx (MotiveList.cpp:254-263): the first row equal
+    to row i in every field."""
+    return int(np.flatnonzero((motl == motl[i]).all(axis=1))[0])
+
+
+def group_count(motl, mode):
+    """MotiveList::GetGroupCount (MotiveList.cpp:233-245): the distinct
+    classNo values for ByGroup, one group per particle otherwise."""
+    if mode == "ByGroup":
+        return len(dict.fromkeys(motl[:, 19].tolist()))
+    return motl.shape[0]
+
+
+def group_members(motl, group, mode, max_distance=0.0, group_size=1):
+    """MotiveList::GetNeighbours(index, mode, maxDist, groupSize)
+    (MotiveList.cpp:132-230): the rows of a group, its leader first.
+    ByGroup: the particles of the group-th classNo in order of first
+    appearance; MaxDistance: the particle, then every other within
+    max_distance in row order; MaxCount: the group_size nearest particles,
+    ordered by (distance, row)."""
+    n = motl.shape[0]
+    if mode == "ByGroup":
+        classes = list(dict.fromkeys(motl[:, 19].tolist()))
+        if group < 0 or group >= len(classes):
+            return []
+        return [i for i in range(n) if motl[i, 19] == classes[group]]
+    if mode == "MaxDistance":
+        md = np.float32(max_distance)
+        return [group] + [i for i in range(n) if i != group and _distance(motl[i], motl[group]) <= md]
+    if mode == "MaxCount":
+        order = sorted((float(_distance(motl[i], motl[group])), i) for i in range(n))
+        return [i for _, i in order[:min(group_size, n)]]
+    raise ValueError(f"GroupMode {mode!r}")
+
+
+def support_members(leader, support_lists, max_distance):
+    """MotiveList::GetNeighbours(index, maxDist, supporters)
+    (MotiveList.cpp:184-205): (list number, row) of every supporting particle
+    within max_distance of the leader."""
+    md = np.float32(max_distance)
+    return [(s, j) for s, lst in enumerate(support_lists) for j in range(lst.shape[0])
+            if _distance(lst[j], leader) <= md]
+
+
+def _remove_radius(size, cfg):
+    """The half width EmSartRefine passes to Volume::RemoveSubVolume: size /
+    (VoxelSize.x / VoxelSizeSubVol) / 2 in float, truncated."""
+    adjust = np.float32(np.float32(cfg.VoxelSize[0]) / np.float32(cfg.VoxelSizeSubVol))
+    return int(np.float32(np.float32(size) / adjust) / np.float32(2.0))
+
+
+def _remove_subvolume(vol, m, radius, saved):
+    """Volume::RemoveSubVolume (Volume.cpp:565-645) at the particle's
+    position + shift (float sum truncated to int, 1-based): zero the cube of
+    half width radius, keeping its contents in `saved`."""
+    dims = vol.shape[::-1]
+    lo = [int(np.float32(m[7 + k] + m[10 + k])) - 1 - radius for k in range(3)]
+    box = [(max(lo[k], 0), min(lo[k] + 2 * radius, dims[k])) for k in range(3)]
+    if any(b[1] <= b[0] for b in box):
+        return
+    region = vol[box[2][0]:box[2][1], box[1][0]:box[1][1], box[0][0]:box[0][1]]
+    saved.append((region, region.clone()))
+    region.zero_()
+
+
+def _cc_shift(R, vg, i, c_full, vol, roi, model, bufs, max_shift, multi, maps):
     """GetDisplacement of projection i (EmSartRefine.cpp:825-980): the
-    compare image of the holey reconstruction's projection against the
-    model's projection. Returns the shift (x, y) as the ShiftFile stores it."""
-    residual, model, mdist = bufs
+    compare image of the holey reconstruction's projection over the group's
+    region against the group's model projection. Returns the shift (x, y) as
+    the ShiftFile stores it."""
+    residual, _ = bufs
     rec = R.rec
     pv, dv, _ = rec.views()
     rec.reset_projections()
     E.forward_project(c_full, vol, pv, dv, roi=roi, fast=True)
     rec.compare(vg, R.prepared[i], i)
     residual.copy_(pv)
-    model.zero_()
-    mdist.zero_()
-    E.forward_project(c_sub, rot, model, mdist, roi=roi, fast=True)
     cmap, cmulti = maps
     (sx, sy), _ = rec.cc_displacement(residual, model, max_shift, multi, cmap, cmulti)
     return sx, sy
@@ -116,13 +187,24 @@ def _cc_shift(R, vg, i, c_full, vol, c_sub, rot, roi, bufs, max_shift, multi, ma
 def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, particles=None, method: str = "cc"):
     """Extra shifts [projection][motive][2] of every particle (the layout
     `fileio.read_shift_file` returns); written to cfg.ShiftOutputFile when
-    `write`. particles: motive list rows to refine (default all); the other
-    rows keep zero shifts. Projections marked unusable in the marker file and
-    particles whose region misses a projection keep zero shifts there.
+    `write`.
+
+    The groups of cfg.GroupMode (EmSartRefine.cpp:697-1090): each group's
+    particles (and the supporting particles within MaxDistanceSupport of its
+    leader) are cut out of the reconstruction and their rotated references
+    projected together as the model; the measured shift goes to every member
+    (ByGroup) or to the leader and the members within SpeedUpDistance of it
+    (MaxDistance, MaxCount; a particle that received a shift is not a leader
+    later). particles: the group numbers to process (default all; rows of
+    the motive list for MaxDistance and MaxCount). Projections marked
+    unusable in the marker file and groups whose region misses a projection
+    keep zero shifts there.
+
     method: "cc" (the reference's cross-correlation peak, integer shifts;
     (-1000, -1000) stored where no positive correlation is found, which
-    EmSARTSubVolumes then leaves out) or "lsq" (sub-pixel least squares;
-    iterations bounds its Gauss-Newton steps)."""
+    EmSARTSubVolumes then leaves out) or "lsq" (sub-pixel least squares, for
+    groups of one particle without supporting particles; iterations bounds
+    its Gauss-Newton steps)."""
     import torch
 
     if method not in ("cc", "lsq"):
@@ -134,74 +216,134 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
     if volf.shape != dims[::-1]:
         raise ValueError(f"{cfg.OutVolumeFile}: volume {volf.shape[::-1]} does not match RecDimensions {dims}")
     # Volume::LoadFromFile negates what it reads (EmSart wrote the volume
-    # negated, Volume::Invert); so does it for the Reference
+    # negated, Volume::Invert); so it does for the references
     vol = torch.from_numpy(np.ascontiguousarray(-volf.astype(np.float32))).to(dev)
     S = cfg.SizeSubVol
-    reff, _ = F.read_em(cfg.Reference)
-    if reff.shape != (S, S, S):
-        raise ValueError(f"{cfg.Reference}: reference {reff.shape} is not SizeSubVol^3 = {S}^3")
-    ref = torch.from_numpy(np.ascontiguousarray(-reff.astype(np.float32))).to(dev)
-    rot = torch.empty_like(ref)
+
+    def load_reference(path, size=None):
+        r, _ = F.read_em(path)
+        if size is not None and r.shape != (size, size, size):
+            raise ValueError(f"{path}: reference {r.shape} is not SizeSubVol^3 = {size}^3")
+        if len(set(r.shape)) != 1:
+            raise ValueError(f"{path}: reference {r.shape} is not a cube")
+        return torch.from_numpy(np.ascontiguousarray(-r.astype(np.float32))).to(dev)
+
+    ref = load_reference(cfg.Reference, S)
+    sup_refs = [load_reference(pth) for pth in cfg.SupportingReferences]
     motl = F.read_motive_list(cfg.MotiveList, cfg.ScaleMotivelistPosition, cfg.ScaleMotivelistShift)
+    sup_lists = [F.read_motive_list(pth, cfg.ScaleMotivelistPosition, cfg.ScaleMotivelistShift)
+                 for pth in cfg.SupportingMotiveLists]
+    if len(sup_lists) < len(sup_refs):
+        raise ValueError("every supporting reference needs its supporting motive list")
     n_part, n_proj = motl.shape[0], len(R.tilt)
     index_list = E.projection_index_list(E.PLT_NORMAL, R.tilt, R.good.astype(np.int32))
     vs = np.array(cfg.VoxelSize, np.float64)
-    radius = int(S / (cfg.VoxelSize[0] / cfg.VoxelSizeSubVol) / 2)  # RemoveSubVolume's half width
     safe = int(100 + cfg.VoxelSizeSubVol * S * 2 + cfg.MaxShift * 2)  # EmSartRefine's safeDist
+    extra = np.zeros((n_proj, n_part, 2), np.float32)
+    max_shift = int(cfg.MaxShift)
+    multi = bool(cfg.MultiPeakDetection)
+    mode = cfg.GroupMode
+    speed_up = np.float32(cfg.SpeedUpDistance)
+    dump = method == "cc" and len(cfg.CCMapFileName) > 3
+    cc_maps, cc_multi = {}, {}
+    model = torch.zeros((H, W), device=dev)
+    mdist = torch.zeros((H, W), device=dev)
+    bufs = (torch.zeros((H, W), device=dev), mdist)
+    cmap = torch.zeros((4 * max_shift, 4 * max_shift), device=dev) if dump else None
+    cmulti = torch.zeros((4 * max_shift, 4 * max_shift), device=dev) if dump and multi else None
     proj = torch.zeros((H, W), device=dev)
     dist = torch.zeros((H, W), device=dev)
     target = torch.zeros((H, W), device=dev)
     out = torch.zeros(8, dtype=torch.float64, device=dev)
-    extra = np.zeros((n_proj, n_part, 2), np.float32)
-    max_shift = int(cfg.MaxShift)
-    multi = bool(cfg.MultiPeakDetection)
-    dump = method == "cc" and len(cfg.CCMapFileName) > 3
-    cc_maps, cc_multi = {}, {}
-    if method == "cc":
-        bufs = (torch.zeros((H, W), device=dev), torch.zeros((H, W), device=dev), torch.zeros((H, W), device=dev))
-        cmap = torch.zeros((4 * max_shift, 4 * max_shift), device=dev) if dump else None
-        cmulti = torch.zeros((4 * max_shift, 4 * max_shift), device=dev) if dump and multi else None
-    for p in (range(n_part) if particles is None else particles):
-        m = motl[p]
-        E.rotate_volume(ref, rot, E.rotation_matrix(m[16], m[17], m[18]))
-        sub = E.subvolume_geometry(S, cfg.VoxelSizeSubVol, vg, m[7:10], m[10:13])
-        # Volume::RemoveSubVolume at the particle's position + shift (as int)
-        lo = [int(m[7 + k] + m[10 + k]) - 1 - radius for k in range(3)]
-        box = [(max(lo[k], 0), min(lo[k] + 2 * radius, dims[k])) for k in range(3)]
-        region = vol[box[2][0]:box[2][1], box[1][0]:box[1][1], box[0][0]:box[0][1]]
-        saved = region.clone()
-        region.zero_()
+    processed = np.zeros(n_part, bool)
+    n_groups = group_count(motl, mode)
+    for group in (range(n_groups) if particles is None else particles):
+        members = group_members(motl, group, mode, cfg.MaxDistance, cfg.GroupSize)
+        if not members:
+            continue
+        lead = global_index(motl, members[0])
+        if mode in ("MaxCount", "MaxDistance") and processed[lead]:
+            continue
+        support = support_members(motl[lead], sup_lists[:len(sup_refs)], cfg.MaxDistanceSupport) if sup_refs else []
+        if method == "lsq" and (len(members) > 1 or support):
+            raise ValueError("method 'lsq' fits groups of one particle without supporting particles")
+        # the particles' rotated references and their boxes; the holey volume
+        saved = []
+        parts = []
+        for k in members:
+            m = motl[k]
+            rot = torch.empty_like(ref)
+            E.rotate_volume(ref, rot, E.rotation_matrix(m[16], m[17], m[18]))
+            parts.append((m, rot, E.subvolume_geometry(S, cfg.VoxelSizeSubVol, vg, m[7:10], m[10:13])))
+            _remove_subvolume(vol, m, _remove_radius(S, cfg), saved)
+        for s_idx, j in support:
+            m = sup_lists[s_idx][j]
+            sref = sup_refs[s_idx]
+            rot = torch.empty_like(sref)
+            E.rotate_volume(sref, rot, E.rotation_matrix(m[16], m[17], m[18]))
+            size = sref.shape[0]
+            parts.append((m, rot, E.subvolume_geometry(size, cfg.VoxelSizeSubVol, vg, m[7:10], m[10:13])))
+            _remove_subvolume(vol, m, _remove_radius(size, cfg), saved)
         for i in index_list:
             i = int(i)
             c_full = E.set_constant_values(R.pg[i], vg)
-            roi = _particle_roi(c_full, m, vg, vs, safe, W, H)
-            x0, y0, x1, y1 = roi
+            # the model: every particle projected over its own region; the
+            # reconstruction over the union of the regions
+            model.zero_()
+            x0, y0, x1, y1 = W, H, 0, 0
+            for m, rot, sub in parts:
+                r = _particle_roi(c_full, m, vg, vs, safe, W, H)
+                if r[2] <= r[0] or r[3] <= r[1]:
+                    continue
+                x0, y0, x1, y1 = min(x0, r[0]), min(y0, r[1]), max(x1, r[2]), max(y1, r[3])
+                if method == "cc":
+                    mdist.zero_()
+                    E.forward_project(E.set_constant_values(R.pg[i], sub), rot, model, mdist, roi=r, fast=True)
             if x1 <= x0 or y1 <= y0:
                 continue
-            c_sub = E.set_constant_values(R.pg[i], sub)
+            roi = (x0, y0, x1, y1)
             if method == "cc":
-                sx, sy = _cc_shift(R, vg, i, c_full, vol, c_sub, rot, roi, bufs, max_shift, multi, (cmap, cmulti))
-                extra[i, p] = (-sx, -sy)  # the file holds the shift; the extra shift is its negation
+                sx, sy = _cc_shift(R, vg, i, c_full, vol, roi, model, bufs, max_shift, multi, (cmap, cmulti))
+                shift = np.array([-sx, -sy], np.float32)  # the file holds the shift; the extra shift is its negation
                 if dump:
                     cc_maps.setdefault(i, []).append(cmap.cpu().numpy().copy())
                     if multi:
                         cc_multi.setdefault(i, []).append(cmulti.cpu().numpy().copy())
-                continue
-            proj.zero_()
-            E.forward_project(c_full, vol, proj, dist, roi=roi, fast=True)
-            target.zero_()
-            target[y0:y1, x0:x1] = R.prepared[i][y0:y1, x0:x1] - proj[y0:y1, x0:x1]
-            s = _fit_shift(c_sub, rot, target, roi, iterations, float(cfg.MaxShift), out)
-            if s is not None:
+            else:
+                m, rot, sub = parts[0]
+                proj.zero_()
+                E.forward_project(c_full, vol, proj, dist, roi=roi, fast=True)
+                target.zero_()
+                target[y0:y1, x0:x1] = R.prepared[i][y0:y1, x0:x1] - proj[y0:y1, x0:x1]
+                s = _fit_shift(E.set_constant_values(R.pg[i], sub), rot, target, roi, iterations,
+                               float(cfg.MaxShift), out)
+                if s is None:
+                    continue
                 # the fitted model moves the particle's image by -s; the
                 # extra shift that moves it back is -s
-                extra[i, p] = -s
-        region.copy_(saved)
+                shift = (-s).astype(np.float32)
+            # EmSartRefine.cpp:1024-1086: the group's shift to its particles
+            if mode == "ByGroup":
+                for k in members:
+                    extra[i, global_index(motl, k)] = shift
+            else:
+                min_dist = np.full(n_part, 1.0e8, np.float32)
+                for k in members[1:]:
+                    g2 = global_index(motl, k)
+                    d = _distance(motl[members[0]], motl[k])
+                    if d <= speed_up and d < min_dist[g2]:
+                        extra[i, g2] = shift
+                        processed[g2] = True
+                        min_dist[g2] = d
+                extra[i, lead] = shift
+                processed[lead] = True
+        for region, keep in reversed(saved):
+            region.copy_(keep)
     if write:
         # the file holds the measured displacement (ShiftFile::SetValue);
         # EmSARTSubVolumes reads it negated as the extra shift
         F.write_shift_file(cfg.ShiftOutputFile, np.moveaxis(-extra, -1, 0))
-        # one slice per refined particle (EmSartRefine.cpp:986-1010)
+        # one slice per group (EmSartRefine.cpp:986-1010)
         for i, maps in cc_maps.items():
             F.write_em(f"{cfg.CCMapFileName}{i}.em", np.stack(maps))
         for i, maps in cc_multi.items():

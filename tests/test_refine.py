@@ -151,10 +151,13 @@ def test_projection_loss_grad_roi_matches_full_image():
         np.testing.assert_allclose(host(o8)[6:], [(pd * pd).sum(), (pd * meas).sum()], rtol=1e-6)
 
 
-def _refine_dataset(tmp_path, bad=None):
+def _refine_dataset(tmp_path, bad=None, layout="single"):
     """Background phantom with the particle cubes zeroed, plus three rotated
     references projected with known extra shifts; files as EmSart and
-    EmSartRefine read them."""
+    EmSartRefine read them. layout "single": one group per particle
+    (MaxCount 1); "group": particles 0 and 1 form one class (ByGroup) and
+    share their extra shifts; "support": as "group", with particle 2 moved
+    to a supporting motive list and shifted with the group."""
     import torch
 
     import artiatomi_b200 as E
@@ -171,6 +174,10 @@ def _refine_dataset(tmp_path, bad=None):
     pos = np.array([[26.0, 28.0, 16.0], [70.0, 66.0, 17.0], [28.0, 70.0, 15.0]], np.float32)
     angles = np.array([[10.0, 35.0, 70.0], [200.0, 15.0, 45.0], [0.0, 90.0, 30.0]], np.float32)
     es = rng.uniform(-1.5, 1.5, size=(n, 3, 2)).astype(np.float32)  # [projection][motive][2]
+    if layout != "single":
+        es[:, 1] = es[:, 0]
+    if layout == "support":
+        es[:, 2] = es[:, 0]
     back = PH.phantom_numpy(dims, 12, seed=2)
     r = S // 2
     for p in range(3):  # Volume::RemoveSubVolume's cube of each particle
@@ -206,6 +213,10 @@ def _refine_dataset(tmp_path, bad=None):
     motl[:, 3] = np.arange(1, 4)
     motl[:, 7:10] = pos
     motl[:, 16:19] = angles
+    motl[:, 19] = (1, 1, 2) if layout != "single" else (1, 2, 3)
+    if layout == "support":
+        F.write_motive_list(str(tmp_path / "support.em"), motl[2:])
+        motl = motl[:2]
     F.write_motive_list(str(tmp_path / "motl.em"), motl)
     cfg = f"""ProjectionFile = {tmp_path / 'ts.mrc'}
 OutVolumeFile = {tmp_path / 'vol.em'}
@@ -239,15 +250,16 @@ MotiveList = {tmp_path / 'motl.em'}
 Reference = {tmp_path / 'ref.em'}
 MaxShift = 3
 ShiftOutputFile = {tmp_path / 'shifts.em'}
-GroupMode = MaxCount
-GroupSize = 1
+{"GroupMode = MaxCount" + chr(10) + "GroupSize = 1" if layout == "single" else "GroupMode = ByGroup"}
+{"" if layout != "support" else "SupportingReferences = " + str(tmp_path / "ref.em") + chr(10)
+ + "SupportingMotiveLists = " + str(tmp_path / "support.em") + chr(10) + "MaxDistanceSupport = 1000"}
 SpeedUpDistance = 0
 ScaleMotivelistShift = 1
 ScaleMotivelistPosition = 1
 MultiPeakDetection = false
 """
     (tmp_path / "refine.cfg").write_text(cfg)
-    return es
+    return es if layout != "support" else es[:, :2]
 
 
 @pytest.mark.gpu
@@ -312,3 +324,85 @@ def test_refine_cc_recovers_integer_shifts(tmp_path, multi):
                 assert (x - c, y - c) == (-got[i, p, 0], -got[i, p, 1])
         if multi:
             assert F.read_em(str(tmp_path / f"ccmap_Multi_{i}.em"))[0].shape == (3, 4 * S, 4 * S)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", ["group", "support"])
+def test_refine_cc_groups(tmp_path, layout):
+    """ByGroup: the two particles of a class are measured together and both
+    get the group's shift; with a supporting particle (its own motive list
+    and reference) its projection joins the model."""
+    from artiatomi_b200.config import EmSartConfig
+    from artiatomi_b200.refine import refine_shifts
+
+    es = _refine_dataset(tmp_path, layout=layout)
+    cfg = EmSartConfig.from_file(str(tmp_path / "refine.cfg"), refine=True)
+    assert cfg.GroupMode == "ByGroup"
+    assert len(cfg.SupportingReferences) == (layout == "support")
+    got = refine_shifts(cfg)
+    assert got.shape == es.shape
+    np.testing.assert_array_equal(got[:, 0], got[:, 1])
+    err = np.abs(got - es)
+    assert err.max() <= 0.6 and err.mean() <= 0.35, (err, got, es)
+
+
+def _motl(coords, classes):
+    m = np.zeros((len(coords), 20), np.float32)
+    m[:, 3] = np.arange(1, len(coords) + 1)
+    m[:, 7:10] = np.asarray(coords, np.float32)
+    m[:, 19] = classes
+    return m
+
+
+def test_group_members_follow_motive_list_rules():
+    """MotiveList::GetNeighbours / GetGroupCount: classes in order of first
+    appearance; MaxDistance: the particle, then the others within the
+    distance in row order; MaxCount: nearest first, ties by row (a particle
+    with equal coordinates and a lower row leads its twin's group)."""
+    from artiatomi_b200 import refine as RF
+
+    coords = [(0, 0, 0), (10, 0, 0), (0, 3, 4), (0, 0, 5), (10, 0, 0), (30, 0, 0)]
+    m = _motl(coords, (5, 2, 5, 7, 2, 5))
+    assert RF.group_count(m, "ByGroup") == 3
+    assert [RF.group_members(m, g, "ByGroup") for g in range(3)] == [[0, 2, 5], [1, 4], [3]]
+    assert RF.group_members(m, 3, "ByGroup") == []
+    assert RF.group_count(m, "MaxCount") == RF.group_count(m, "MaxDistance") == 6
+    assert RF.group_members(m, 3, "MaxDistance", max_distance=5.0) == [3, 0, 2]
+    assert RF.group_members(m, 0, "MaxCount", group_size=3) == [0, 2, 3]  # distances 0, 5, 5
+    assert RF.group_members(m, 4, "MaxCount", group_size=2) == [1, 4]  # twin of row 1
+    assert RF.group_members(m, 5, "MaxCount", group_size=99) == [5, 1, 4, 0, 2, 3]
+    assert RF.global_index(m, 4) == 4  # rows differ in the particle number
+    twin = m.copy()
+    twin[4] = twin[1]
+    assert RF.global_index(twin, 4) == 1
+
+
+def test_support_members_and_remove_radius():
+    from artiatomi_b200 import refine as RF
+    from artiatomi_b200.config import EmSartConfig
+
+    lead = _motl([(0, 0, 0)], (1,))[0]
+    s0 = _motl([(3, 4, 0), (30, 0, 0)], (1, 1))
+    s1 = _motl([(0, 0, 5.5)], (1,))
+    assert RF.support_members(lead, [s0, s1], 5.0) == [(0, 0)]
+    assert RF.support_members(lead, [s0, s1], 6.0) == [(0, 0), (1, 0)]
+    cfg = EmSartConfig()
+    cfg.VoxelSize, cfg.VoxelSizeSubVol = (4.0, 4.0, 4.0), 1.0
+    assert RF._remove_radius(64, cfg) == 8  # 64 / 4 / 2
+    cfg.VoxelSize, cfg.VoxelSizeSubVol = (3.0, 3.0, 3.0), 2.0
+    assert RF._remove_radius(33, cfg) == 11  # 33 / 1.5 / 2 = 11.0
+    assert RF._remove_radius(35, cfg) == 11  # 11.67 truncated
+
+
+def test_refine_config_supporting_lists():
+    from artiatomi_b200.config import EmSartConfig
+    from tests.test_fileio import CFG
+
+    c = EmSartConfig.from_text(CFG + REFINE_KEYS + "SupportingReferences = /d/a.em;/d/b.em;x;\n"
+                               "SupportingMotiveLists = /d/ma.em;/d/mb.em\nMaxDistanceSupport = 40\n", refine=True)
+    assert c.SupportingReferences == ["/d/a.em", "/d/b.em"]
+    assert c.SupportingMotiveLists == ["/d/ma.em", "/d/mb.em"]
+    assert c.MaxDistanceSupport == 40.0
+    with pytest.raises(KeyError):
+        EmSartConfig.from_text(CFG + REFINE_KEYS + "SupportingReferences = /d/a.em\n", refine=True)
+    assert EmSartConfig.from_text(CFG + REFINE_KEYS, refine=True).SupportingReferences == []
