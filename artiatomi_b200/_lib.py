@@ -119,6 +119,7 @@ _SIGS = {
     "esb_prepare_projection": ([P, C.POINTER(PrepareConfig), P, P, C.POINTER(F), C.POINTER(F), C.POINTER(I)], I),
     "esb_rec_cc_displacement": ([P, P, P, I, I, P, C.POINTER(F), P, P], I),
     "esb_rec_forward_projection": ([P, C.POINTER(VolGeom), P, I, I, I], I),
+    "esb_rec_forward_projection_roi": ([P, C.POINTER(VolGeom), P, I, I, I, P], I),
     "esb_rec_compare": ([P, C.POINTER(VolGeom), P, I], I),
     "esb_rec_back_projection": ([P, C.POINTER(VolGeom), P, I, I, F], I),
     "esb_sart_run": ([P, C.POINTER(VolGeom), P, I, P, P, I, I, I, C.POINTER(I)], I),

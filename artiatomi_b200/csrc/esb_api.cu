@@ -863,19 +863,21 @@ static BpShape rec_bp_shape(esb_reconstructor* r, const KConst& c, int vt, const
 }
 
 // Kernel variant of the reconstructor (faithful or fast).
-static cudaError_t rec_march(esb_reconstructor* r, const KConst& c, const void* vol, int vt) {
-  const int W = r->cfg.proj_x, H = r->cfg.proj_y;
+// roi: detector region [roi[0], roi[2]) x [roi[1], roi[3]) (the reference's
+// roiMin / roiMax), already clipped to the image.
+static cudaError_t rec_march(esb_reconstructor* r, const KConst& c, const void* vol, int vt, const int* roi) {
+  const int W = r->cfg.proj_x;
   if (r->cfg.variant == ESB_VARIANT_FAST)
-    return launch_project_fast(c, vol, vt, 0, r->proj_d, r->dist_d, W, 0.f, 0.f, 0, 0, W, H, r->stream,
-                               rec_march_nw(r, c, vol, vt));
-  return launch_march(c, vol, vt, r->proj_d, r->dist_d, W, 0, 0, W, H, r->stream);
+    return launch_project_fast(c, vol, vt, 0, r->proj_d, r->dist_d, W, 0.f, 0.f, roi[0], roi[1], roi[2], roi[3],
+                               r->stream, rec_march_nw(r, c, vol, vt));
+  return launch_march(c, vol, vt, r->proj_d, r->dist_d, W, roi[0], roi[1], roi[2], roi[3], r->stream);
 }
 static cudaError_t rec_slicer(esb_reconstructor* r, const KConst& c, const void* vol, int vt, float* out, float t0,
-                              float t1) {
-  const int W = r->cfg.proj_x, H = r->cfg.proj_y;
+                              float t1, const int* roi) {
+  const int W = r->cfg.proj_x;
   if (r->cfg.variant == ESB_VARIANT_FAST)
-    return launch_project_fast(c, vol, vt, 1, out, nullptr, W, t0, t1, 0, 0, W, H, r->stream);
-  return launch_slicer(c, vol, vt, out, W, t0, t1, 0, 0, W, H, r->stream);
+    return launch_project_fast(c, vol, vt, 1, out, nullptr, W, t0, t1, roi[0], roi[1], roi[2], roi[3], r->stream);
+  return launch_slicer(c, vol, vt, out, W, t0, t1, roi[0], roi[1], roi[2], roi[3], r->stream);
 }
 static cudaError_t rec_bp(esb_reconstructor* r, const KConst& c, void* vol, int vt, const float* img, float lambda,
                           float dmin, float dmax, int linear) {
@@ -1093,24 +1095,34 @@ static const float* rec_upsample(esb_reconstructor* r, const KConst& c, int coun
   return r->up_imgs;
 }
 
-extern "C" {
-
-int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, const void* vol, int voxel_type, int index,
-                               int volume_is_empty) {
+// ForwardProjection / ForwardProjectionROI (Reconstructor.cpp:428-644,
+// 649-859): rays of the detector region roi (NULL: the whole detector) are
+// projected and added to proj_d; dist_d gets their traversal lengths. With
+// CTF every slab image is filtered over the whole detector.
+static int rec_forward(esb_reconstructor* r, const esb_vol_geom* vg, const void* vol, int voxel_type, int index,
+                       int volume_is_empty, const int* roi_in, const char* where) {
   int rc;
-  if ((rc = rec_check(r, vg, index, "esb_rec_forward_projection"))) return rc;
-  if (!vol || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_forward_projection: invalid volume");
+  if ((rc = rec_check(r, vg, index, where))) return rc;
+  if (!vol || !valid_vt(voxel_type)) return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": invalid volume");
   const esb_recon_config& cf = r->cfg;
   const int W = cf.proj_x, H = cf.proj_y;
+  int roi[4] = {0, 0, W, H};
+  if (roi_in) {
+    roi[0] = std::max(roi_in[0], 0);
+    roi[1] = std::max(roi_in[1], 0);
+    roi[2] = std::min(roi_in[2], W);
+    roi[3] = std::min(roi_in[3], H);
+    if (roi[2] <= roi[0] || roi[3] <= roi[1]) return ok();  // no ray in the region
+  }
   KConst c = rec_const(r, r->geoms[index], *vg, 0);
   if (volume_is_empty) {  // Reconstructor.cpp:465-470 / 622-627
     PhaseScope ps(r, 0);
-    ESB_CK(launch_travlen(c, r->dist_d, W, 0, 0, W, H, r->stream), "esb_rec_forward_projection");
+    ESB_CK(launch_travlen(c, r->dist_d, W, roi[0], roi[1], roi[2], roi[3], r->stream), where);
     return ok();
   }
   if (!cf.ctf_mode) {  // ForwardProjectionNoCTF (Reconstructor.cpp:429-438)
     PhaseScope ps(r, 0);
-    ESB_CK(rec_march(r, c, vol, voxel_type), "esb_rec_forward_projection");
+    ESB_CK(rec_march(r, c, vol, voxel_type, roi), where);
     return ok();
   }
   // ForwardProjectionCTF (Reconstructor.cpp:496-590)
@@ -1127,13 +1139,14 @@ int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, con
     {
       PhaseScope ps(r, 3);
       ESB_CK(cudaMemsetAsync(r->slab_imgs, 0, (size_t)T.count * img * sizeof(float), r->stream),
-             "esb_rec_forward_projection");
+             where);
     }
     {
       PhaseScope ps(r, 0);
       const int nw = rec_slicer_nw(r, c, vol, voxel_type, img, T);
-      ESB_CK(launch_slicer_fused(c, vol, voxel_type, r->slab_imgs, img, W, T, 0, 0, W, H, r->stream, nw),
-             "esb_rec_forward_projection");
+      ESB_CK(launch_slicer_fused(c, vol, voxel_type, r->slab_imgs, img, W, T, roi[0], roi[1], roi[2], roi[3],
+                                 r->stream, nw),
+             where);
     }
     // each slab image through the CTF, added to proj_d in slab order
     if ((rc = rec_ctf_chain_slabs(r, T, index, r->slab_imgs, 0, 1, full, 1, nullptr, r->proj_d, 1, full, 0))) return rc;
@@ -1145,21 +1158,34 @@ int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, con
                         cf.switch_ctf_direction, &dmin, &dmax);
     {
       PhaseScope ps(r, 3);
-      ESB_CK(cudaMemsetAsync(r->dist_d, 0, (size_t)W * H * sizeof(float), r->stream), "esb_rec_forward_projection");
+      ESB_CK(cudaMemsetAsync(r->dist_d, 0, (size_t)W * H * sizeof(float), r->stream), where);
     }
     {
       PhaseScope ps(r, 0);
-      ESB_CK(rec_slicer(r, c, vol, voxel_type, r->dist_d, ray, ray + step), "esb_rec_forward_projection");
+      ESB_CK(rec_slicer(r, c, vol, voxel_type, r->dist_d, ray, ray + step, roi), where);
     }
     if ((rc = rec_ctf_chain(r, r->dist_d, 1, full, index, dmin, dmax, 1, nullptr, r->proj_d, 1, full))) return rc;
   }
   {
     PhaseScope ps(r, 3);
-    ESB_CK(cudaMemsetAsync(r->dist_d, 0, (size_t)W * H * sizeof(float), r->stream), "esb_rec_forward_projection");
+    ESB_CK(cudaMemsetAsync(r->dist_d, 0, (size_t)W * H * sizeof(float), r->stream), where);
   }
   PhaseScope ps(r, 0);
-  ESB_CK(launch_travlen(c, r->dist_d, W, 0, 0, W, H, r->stream), "esb_rec_forward_projection");
+  ESB_CK(launch_travlen(c, r->dist_d, W, roi[0], roi[1], roi[2], roi[3], r->stream), where);
   return ok();
+}
+
+extern "C" {
+
+int esb_rec_forward_projection(esb_reconstructor* r, const esb_vol_geom* vg, const void* vol, int voxel_type, int index,
+                               int volume_is_empty) {
+  return rec_forward(r, vg, vol, voxel_type, index, volume_is_empty, nullptr, "esb_rec_forward_projection");
+}
+
+int esb_rec_forward_projection_roi(esb_reconstructor* r, const esb_vol_geom* vg, const void* vol, int voxel_type,
+                                   int index, int volume_is_empty, const int roi[4]) {
+  if (!roi) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_rec_forward_projection_roi: roi is NULL");
+  return rec_forward(r, vg, vol, voxel_type, index, volume_is_empty, roi, "esb_rec_forward_projection_roi");
 }
 
 int esb_rec_compare(esb_reconstructor* r, const esb_vol_geom* vg, const float* real, int index) {

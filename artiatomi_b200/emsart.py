@@ -501,6 +501,13 @@ class Reconstructor:
         check(lib.esb_rec_forward_projection(self._h, C.byref(vg), fptr(vol), _voxel_type_of(vol), index,
                                              int(volume_is_empty)))
 
+    def forward_projection_roi(self, vg, vol, index: int, roi, volume_is_empty: bool = False):
+        """ForwardProjectionROI: the rays of detector region roi = (x0, y0,
+        x1, y1) (x1, y1 exclusive), added to the projection buffer."""
+        r = np.ascontiguousarray(np.asarray(roi, np.int32))
+        check(lib.esb_rec_forward_projection_roi(self._h, C.byref(vg), fptr(vol), _voxel_type_of(vol), index,
+                                                 int(volume_is_empty), fptr(r)))
+
     def compare(self, vg, real, index: int):
         check(lib.esb_rec_compare(self._h, C.byref(vg), fptr(real), index))
 

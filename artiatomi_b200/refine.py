@@ -28,7 +28,9 @@ fitted to the residual (prepared projection minus the reconstruction's
 projection) with a detector offset s, min over (alpha, s) of
 1/2 ||alpha A(ref, s) - r||^2, Gauss-Newton on s
 (esb_projection_loss_grad_roi) with the amplitude alpha in closed form: a
-sub-pixel estimate. Both use the projector without the CTF of CtfMode.
+sub-pixel estimate. Method "cc" projects through the reconstructor
+(ForwardProjectionROI, with the per-slab CTF in CtfMode); method "lsq" uses
+the plain ray integrals.
 
 Every computation runs in the library's CUDA kernels; this module moves
 files and buffers and solves the 2 x 2 Gauss-Newton systems.
@@ -167,16 +169,22 @@ def _remove_subvolume(vol, m, radius, saved):
     region.zero_()
 
 
-def _cc_shift(R, vg, i, c_full, vol, roi, model, bufs, max_shift, multi, maps):
+def _cc_shift(R, vg, i, vol, parts_roi, roi, bufs, max_shift, multi, maps):
     """GetDisplacement of projection i (EmSartRefine.cpp:825-980): the
-    compare image of the holey reconstruction's projection over the group's
-    region against the group's model projection. Returns the shift (x, y) as
+    particles' projections (each over its region) are the model; the holey
+    reconstruction's projection over the union region goes through Compare;
+    both through GetDisplacement. Projections are the reconstructor's
+    (ForwardProjectionROI: with CTF in CtfMode). Returns the shift (x, y) as
     the ShiftFile stores it."""
-    residual, _ = bufs
+    residual, model = bufs
     rec = R.rec
-    pv, dv, _ = rec.views()
+    pv, _, _ = rec.views()
     rec.reset_projections()
-    E.forward_project(c_full, vol, pv, dv, roi=roi, fast=True)
+    for sub, rot, r in parts_roi:
+        rec.forward_projection_roi(sub, rot, i, r)
+    model.copy_(pv)  # CopyProjectionToSubVolumeProjection
+    rec.reset_projections()
+    rec.forward_projection_roi(vg, vol, i, roi)
     rec.compare(vg, R.prepared[i], i)
     residual.copy_(pv)
     cmap, cmulti = maps
@@ -246,9 +254,7 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
     speed_up = np.float32(cfg.SpeedUpDistance)
     dump = method == "cc" and len(cfg.CCMapFileName) > 3
     cc_maps, cc_multi = {}, {}
-    model = torch.zeros((H, W), device=dev)
-    mdist = torch.zeros((H, W), device=dev)
-    bufs = (torch.zeros((H, W), device=dev), mdist)
+    bufs = (torch.zeros((H, W), device=dev), torch.zeros((H, W), device=dev))  # residual, model
     cmap = torch.zeros((4 * max_shift, 4 * max_shift), device=dev) if dump else None
     cmulti = torch.zeros((4 * max_shift, 4 * max_shift), device=dev) if dump and multi else None
     proj = torch.zeros((H, W), device=dev)
@@ -289,21 +295,19 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
             c_full = E.set_constant_values(R.pg[i], vg)
             # the model: every particle projected over its own region; the
             # reconstruction over the union of the regions
-            model.zero_()
             x0, y0, x1, y1 = W, H, 0, 0
+            parts_roi = []
             for m, rot, sub in parts:
                 r = _particle_roi(c_full, m, vg, vs, safe, W, H)
                 if r[2] <= r[0] or r[3] <= r[1]:
                     continue
                 x0, y0, x1, y1 = min(x0, r[0]), min(y0, r[1]), max(x1, r[2]), max(y1, r[3])
-                if method == "cc":
-                    mdist.zero_()
-                    E.forward_project(E.set_constant_values(R.pg[i], sub), rot, model, mdist, roi=r, fast=True)
+                parts_roi.append((sub, rot, r))
             if x1 <= x0 or y1 <= y0:
                 continue
             roi = (x0, y0, x1, y1)
             if method == "cc":
-                sx, sy = _cc_shift(R, vg, i, c_full, vol, roi, model, bufs, max_shift, multi, (cmap, cmulti))
+                sx, sy = _cc_shift(R, vg, i, vol, parts_roi, roi, bufs, max_shift, multi, (cmap, cmulti))
                 shift = np.array([-sx, -sy], np.float32)  # the file holds the shift; the extra shift is its negation
                 if dump:
                     cc_maps.setdefault(i, []).append(cmap.cpu().numpy().copy())

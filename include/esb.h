@@ -376,6 +376,15 @@ int esb_rec_reset_projections(esb_reconstructor* rec);
 /* ForwardProjection (Reconstructor.cpp:1411-1421), CTF or not. */
 int esb_rec_forward_projection(esb_reconstructor* rec, const esb_vol_geom* vg, const void* vol, int voxel_type,
                                int index, int volume_is_empty);
+/* ForwardProjectionROI (Reconstructor.cpp:1519-1529 -> ForwardProjectionNoCTFROI
+ * :649-712, ForwardProjectionCTFROI :716-859): ForwardProjection for the rays
+ * of the detector region [roi[0], roi[2]) x [roi[1], roi[3]) only (the
+ * reference's roiMin / roiMax, clipped to the detector), added to the
+ * projection buffer; with CTF each slab image is still filtered over the
+ * whole detector. EmSartRefine projects the particles' models and the
+ * reconstruction without them this way. */
+int esb_rec_forward_projection_roi(esb_reconstructor* rec, const esb_vol_geom* vg, const void* vol, int voxel_type,
+                                   int index, int volume_is_empty, const int roi[4]);
 /* Compare (Reconstructor.cpp:1386-1405). real: device image W x H. */
 int esb_rec_compare(esb_reconstructor* rec, const esb_vol_geom* vg, const float* real, int index);
 /* BackProjection (Reconstructor.cpp:871-887 / 920-969) of proj_d. */
