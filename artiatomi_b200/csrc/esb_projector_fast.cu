@@ -178,14 +178,8 @@ __device__ float layer_sum_xz(const Cell<VT>& C, float qx, float b, int iy, floa
   const Off y0 = (Off)(iy < 0 ? 0 : (iy > C.ny - 1 ? C.ny - 1 : iy)) * (Off)C.sy;
   const Off y1 = (Off)(iy + 1 < 0 ? 0 : (iy + 1 > C.ny - 1 ? C.ny - 1 : iy + 1)) * (Off)C.sy;
   const float ib = 1.0f - b;
-  // the two rows' base pointers: a corner's address is then one multiply-add
-  // of its x-z offset (o + y0 stays below the voxel count, so this is the
-  // same address as the 32-bit sum)
-  typedef typename Voxel<VT>::T Vox;
-  const Vox* __restrict__ row0 = (const Vox*)C.vol + (size_t)y0;
-  const Vox* __restrict__ row1 = (const Vox*)C.vol + (size_t)y1;
   auto ey = [&](Off o) {
-    return ib * Voxel<VT>::load(row0, (long)o) + b * Voxel<VT>::load(row1, (long)o);
+    return ib * Voxel<VT>::load(C.vol, (long)(o + y0)) + b * Voxel<VT>::load(C.vol, (long)(o + y1));
   };
   // original indices of the current cell's near and far corners per axis
   int inF = sn * (int)fcn + sn;
