@@ -170,25 +170,26 @@ def _remove_subvolume(vol, m, radius, saved):
 
 
 def _cc_shift(R, vg, i, vol, parts_roi, roi, bufs, max_shift, multi, maps):
-    """GetDisplacement of projection i (EmSartRefine.cpp:825-980): the
-    particles' projections (each over its region) are the model; the holey
+    """GetDisplacement of projection i (EmSartRefine.cpp:825-980): the holey
     reconstruction's projection over the union region goes through Compare;
-    both through GetDisplacement. Projections are the reconstructor's
-    (ForwardProjectionROI: with CTF in CtfMode). Returns the shift (x, y) as
-    the ShiftFile stores it."""
-    residual, model = bufs
+    the particles' projections (each over its region) are the model; both
+    through GetDisplacement. Projections are the reconstructor's
+    (ForwardProjectionROI: with CTF in CtfMode). bufs: a residual image and
+    the reconstructor's projection buffer. Returns the shift (x, y) as the
+    ShiftFile stores it."""
+    residual, proj = bufs
     rec = R.rec
-    pv, _, _ = rec.views()
-    rec.reset_projections()
-    for sub, rot, r in parts_roi:
-        rec.forward_projection_roi(sub, rot, i, r)
-    model.copy_(pv)  # CopyProjectionToSubVolumeProjection
     rec.reset_projections()
     rec.forward_projection_roi(vg, vol, i, roi)
     rec.compare(vg, R.prepared[i], i)
-    residual.copy_(pv)
+    residual.copy_(proj)
+    rec.reset_projections()
+    for sub, rot, r in parts_roi:
+        rec.forward_projection_roi(sub, rot, i, r)
     cmap, cmulti = maps
-    (sx, sy), _ = rec.cc_displacement(residual, model, max_shift, multi, cmap, cmulti)
+    # the model stays in the projection buffer (the reference copies it to
+    # projSubVols_d first, CopyProjectionToSubVolumeProjection)
+    (sx, sy), _ = rec.cc_displacement(residual, proj, max_shift, multi, cmap, cmulti)
     return sx, sy
 
 
@@ -254,7 +255,7 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
     speed_up = np.float32(cfg.SpeedUpDistance)
     dump = method == "cc" and len(cfg.CCMapFileName) > 3
     cc_maps, cc_multi = {}, {}
-    bufs = (torch.zeros((H, W), device=dev), torch.zeros((H, W), device=dev))  # residual, model
+    bufs = (torch.zeros((H, W), device=dev), R.rec.views()[0])  # residual, the projection buffer
     cmap = torch.zeros((4 * max_shift, 4 * max_shift), device=dev) if dump else None
     cmulti = torch.zeros((4 * max_shift, 4 * max_shift), device=dev) if dump and multi else None
     proj = torch.zeros((H, W), device=dev)

@@ -69,13 +69,13 @@ def main(argv=None):
     R = types.SimpleNamespace(rec=rec, prepared=prepared)
     cfg = types.SimpleNamespace(VoxelSize=(1.0, 1.0, 1.0), VoxelSizeSubVol=1.0)
     safe = int(100 + S * 2 + a.max_shift * 2)
-    bufs = (torch.zeros((W, W), device="cuda"), torch.zeros((W, W), device="cuda"))
+    bufs = (torch.zeros((W, W), device="cuda"), rec.views()[0])
     margin = S // 2 + 2
     pos = np.stack([rng.uniform(margin + 1, d - margin, a.particles) for d in dims], 1).astype(np.float32)
     ang = rng.uniform(0.0, 360.0, (a.particles, 3)).astype(np.float32)
     vs = np.ones(3)
 
-    def particle(p, count_only=False):
+    def particle(p):
         m = np.zeros(20, np.float32)
         m[7:10], m[16:19] = pos[p], ang[p]
         E.rotate_volume(ref, rot, E.rotation_matrix(*ang[p]))
