@@ -7,15 +7,16 @@ usable projection, the particle's extra detector shift. The shifts go to
 ShiftOutputFile in the ShiftFile layout that EmSARTSubVolumes reads as its
 ShiftInputFile (`reconstruct_subvolumes`).
 
-For each particle (EmSartRefine.cpp:700-1100, one particle per group) and
-projection:
-- the reconstruction with the particle's cube zeroed (Volume::RemoveSubVolume,
-  Volume.cpp:565-645) is forward projected over the particle's detector
-  region (ForwardProjectionROI);
-- the Reference, rotated to the particle's Euler angles (esb_rotate_volume,
+For each group of particles (EmSartRefine.cpp:697-1090: GroupMode ByGroup,
+MaxDistance or MaxCount, plus the supporting particles of
+SupportingReferences / SupportingMotiveLists) and projection:
+- the reconstruction with the particles' cubes zeroed
+  (Volume::RemoveSubVolume, Volume.cpp:565-645) is forward projected over
+  the union of the particles' detector regions (ForwardProjectionROI);
+- each particle's reference, rotated to its Euler angles (esb_rotate_volume,
   the reference's rot3d) and placed at the particle (esb_subvolume_geometry),
-  is the model.
-Both volumes are read negated, as Volume::LoadFromFile (Volume.cpp:498-550)
+  is projected over its region; the sum is the model.
+The volumes are read negated, as Volume::LoadFromFile (Volume.cpp:498-550)
 reads every volume (EmSart and EmSARTSubVolumes write theirs negated).
 
 method "cc" (the reference's): the compare image of the reconstruction's
