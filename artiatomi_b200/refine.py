@@ -149,6 +149,39 @@ def support_members(leader, support_lists, max_distance):
             if _distance(lst[j], leader) <= md]
 
 
+def groups(motl, mode, processed, max_distance=0.0, group_size=1, only=None):
+    """The groups EmSartRefine measures, in its order (EmSartRefine.cpp:
+    697-730): (group number, member rows, leader's global index). A MaxCount
+    or MaxDistance group whose leader already received a shift is skipped;
+    `processed` is read as the caller updates it. only: the group numbers
+    to consider (default all)."""
+    for group in (range(group_count(motl, mode)) if only is None else only):
+        members = group_members(motl, group, mode, max_distance, group_size)
+        if not members:
+            continue
+        lead = global_index(motl, members[0])
+        if mode in ("MaxCount", "MaxDistance") and processed[lead]:
+            continue
+        yield group, members, lead
+
+
+def shift_receivers(motl, members, mode, speed_up):
+    """Global indices that get a group's shift in one projection, in the
+    order EmSartRefine.cpp:1024-1086 stores them: every member (ByGroup), or
+    the members within speed_up of the leader and then the leader."""
+    if mode == "ByGroup":
+        return [global_index(motl, k) for k in members]
+    out, min_dist = [], {}  # minDistOfProcessedParticles, reset per projection
+    for k in members[1:]:
+        g2 = global_index(motl, k)
+        d = _distance(motl[members[0]], motl[k])
+        if d <= np.float32(speed_up) and d < min_dist.get(g2, np.float32(1.0e8)):
+            out.append(g2)
+            min_dist[g2] = d
+    out.append(global_index(motl, members[0]))
+    return out
+
+
 def _remove_radius(size, cfg):
     """The half width EmSartRefine passes to Volume::RemoveSubVolume: size /
     (VoxelSize.x / VoxelSizeSubVol) / 2 in float, truncated."""
@@ -264,14 +297,8 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
     target = torch.zeros((H, W), device=dev)
     out = torch.zeros(8, dtype=torch.float64, device=dev)
     processed = np.zeros(n_part, bool)
-    n_groups = group_count(motl, mode)
-    for group in (range(n_groups) if particles is None else particles):
-        members = group_members(motl, group, mode, cfg.MaxDistance, cfg.GroupSize)
-        if not members:
-            continue
-        lead = global_index(motl, members[0])
-        if mode in ("MaxCount", "MaxDistance") and processed[lead]:
-            continue
+    for group, members, lead in groups(motl, mode, processed, cfg.MaxDistance, cfg.GroupSize, particles):
+        receivers = shift_receivers(motl, members, mode, speed_up)
         support = support_members(motl[lead], sup_lists[:len(sup_refs)], cfg.MaxDistanceSupport) if sup_refs else []
         if method == "lsq" and (len(members) > 1 or support):
             raise ValueError("method 'lsq' fits groups of one particle without supporting particles")
@@ -329,20 +356,10 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
                 # extra shift that moves it back is -s
                 shift = (-s).astype(np.float32)
             # EmSartRefine.cpp:1024-1086: the group's shift to its particles
-            if mode == "ByGroup":
-                for k in members:
-                    extra[i, global_index(motl, k)] = shift
-            else:
-                min_dist = np.full(n_part, 1.0e8, np.float32)
-                for k in members[1:]:
-                    g2 = global_index(motl, k)
-                    d = _distance(motl[members[0]], motl[k])
-                    if d <= speed_up and d < min_dist[g2]:
-                        extra[i, g2] = shift
-                        processed[g2] = True
-                        min_dist[g2] = d
-                extra[i, lead] = shift
-                processed[lead] = True
+            for g2 in receivers:
+                extra[i, g2] = shift
+                if mode != "ByGroup":
+                    processed[g2] = True
         for region, keep in reversed(saved):
             region.copy_(keep)
     if write:

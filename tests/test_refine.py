@@ -406,3 +406,34 @@ def test_refine_config_supporting_lists():
     with pytest.raises(KeyError):
         EmSartConfig.from_text(CFG + REFINE_KEYS + "SupportingReferences = /d/a.em\n", refine=True)
     assert EmSartConfig.from_text(CFG + REFINE_KEYS, refine=True).SupportingReferences == []
+
+
+def _visit(m, mode, speed_up, **kw):
+    """Drive refine's group iteration as refine_shifts does when every group
+    gets a shift: (group, receivers) in order."""
+    from artiatomi_b200 import refine as RF
+
+    processed = np.zeros(m.shape[0], bool)
+    seen = []
+    for g, members, lead in RF.groups(m, mode, processed, **kw):
+        rec = RF.shift_receivers(m, members, mode, speed_up)
+        assert rec[-1] == lead or mode == "ByGroup"
+        if mode != "ByGroup":
+            processed[rec] = True
+        seen.append((g, rec))
+    return seen
+
+
+def test_group_iteration_and_speed_up():
+    """EmSartRefine.cpp:697-730 and 1024-1086: a MaxCount / MaxDistance group
+    hands its shift to the members within SpeedUpDistance of its leader, and
+    a particle that received a shift leads no later group; ByGroup hands it
+    to every member and skips nothing."""
+    m = _motl([(0, 0, 0), (1, 0, 0), (10, 0, 0), (10.5, 0, 0), (30, 0, 0)], (1, 1, 2, 2, 3))
+    assert _visit(m, "MaxCount", 2.0, group_size=2) == [(0, [1, 0]), (2, [3, 2]), (4, [4])]
+    assert _visit(m, "MaxCount", 0.5, group_size=2) == [(0, [0]), (1, [1]), (2, [3, 2]), (4, [4])]  # 0.5 <= 0.5
+    assert _visit(m, "MaxCount", 0.4, group_size=2) == [(g, [g]) for g in range(5)]
+    assert _visit(m, "MaxDistance", 1.0, max_distance=1.0) == [(0, [1, 0]), (2, [3, 2]), (4, [4])]
+    assert _visit(m, "MaxDistance", 0.0, max_distance=50.0) == [(g, [g]) for g in range(5)]
+    assert _visit(m, "ByGroup", 0.0) == [(0, [0, 1]), (1, [2, 3]), (2, [4])]
+    assert _visit(m, "MaxCount", 2.0, group_size=2, only=[2, 4]) == [(2, [3, 2]), (4, [4])]
