@@ -166,3 +166,23 @@ def test_cc_displacement_rejects_bad_max_shift():
     for s in (0, 17):
         with pytest.raises(EsbError):
             rec.cc_displacement(cuda(r), cuda(m), s)
+
+
+def test_oracle_correlation_is_the_normalised_circular_correlation():
+    """The FFT route of GetDisplacement (conj(A) B, unnormalised C2R, division
+    by N^2 sqrt(SumA SumB)) against the direct sum
+    cc(s) = sum_x a(x) b(x + s) / sqrt(sum a^2 sum b^2) of the mean-free
+    squares, on a 12 x 12 case without padding."""
+    rng = np.random.default_rng(5)
+    n = 12
+    a = rng.normal(size=(n, n)).astype(np.float32)
+    b = rng.normal(size=(n, n)).astype(np.float32)
+    o = OC.cc_displacement(a, b, n, 0, 0, 3)
+    a0 = a.astype(np.float64) - a.mean(dtype=np.float64)
+    b0 = b.astype(np.float64) - b.mean(dtype=np.float64)
+    direct = np.zeros((n, n))
+    for sy in range(n):
+        for sx in range(n):
+            direct[sy, sx] = (a0 * np.roll(b0, (-sy, -sx), axis=(0, 1))).sum()
+    direct /= np.sqrt((a0 * a0).sum() * (b0 * b0).sum())
+    np.testing.assert_allclose(o["cc"], direct, rtol=0, atol=2e-6)
