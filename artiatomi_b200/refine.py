@@ -210,7 +210,7 @@ def _cc_shift(R, vg, i, vol, parts_roi, roi, bufs, max_shift, multi, maps):
     through GetDisplacement. Projections are the reconstructor's
     (ForwardProjectionROI: with CTF in CtfMode). bufs: a residual image and
     the reconstructor's projection buffer. Returns the shift (x, y) as the
-    ShiftFile stores it."""
+    ShiftFile stores it, and the correlation maximum."""
     residual, proj = bufs
     rec = R.rec
     rec.reset_projections()
@@ -223,8 +223,19 @@ def _cc_shift(R, vg, i, vol, parts_roi, roi, bufs, max_shift, multi, maps):
     cmap, cmulti = maps
     # the model stays in the projection buffer (the reference copies it to
     # projSubVols_d first, CopyProjectionToSubVolumeProjection)
-    (sx, sy), _ = rec.cc_displacement(residual, proj, max_shift, multi, cmap, cmulti)
-    return sx, sy
+    (sx, sy), value = rec.cc_displacement(residual, proj, max_shift, multi, cmap, cmulti)
+    return sx, sy, value
+
+
+def write_relations(path, relations, cc_values):
+    """The `<ShiftOutputFile>.relations` text EmSartRefine writes
+    (EmSartRefine.cpp:1104-1116): per particle "particleNr; particleNrInTomo;
+    particleNrInTomo; obtainedShiftFromID; CCValue" (the second number
+    written twice, as the reference does), integers as ints and the value as
+    a C++ stream formats a float."""
+    with open(path, "w") as f:
+        for r, v in zip(relations, cc_values):
+            f.write(f"{int(r[0])}; {int(r[1])}; {int(r[1])}; {int(r[3])}; {'%g' % float(np.float32(v))}\n")
 
 
 def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, particles=None, method: str = "cc"):
@@ -297,6 +308,10 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
     target = torch.zeros((H, W), device=dev)
     out = torch.zeros(8, dtype=torch.float64, device=dev)
     processed = np.zeros(n_part, bool)
+    # groupRelations per particle: particleNr, particleNrInTomo, tomoNr,
+    # obtainedShiftFromID; and CCValue (EmSartRefine.cpp:74-81, zeroed)
+    relations = np.zeros((n_part, 4), np.int64)
+    rel_cc = np.zeros(n_part, np.float32)
     for group, members, lead in groups(motl, mode, processed, cfg.MaxDistance, cfg.GroupSize, particles):
         receivers = shift_receivers(motl, members, mode, speed_up)
         support = support_members(motl[lead], sup_lists[:len(sup_refs)], cfg.MaxDistanceSupport) if sup_refs else []
@@ -336,7 +351,7 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
                 continue
             roi = (x0, y0, x1, y1)
             if method == "cc":
-                sx, sy = _cc_shift(R, vg, i, vol, parts_roi, roi, bufs, max_shift, multi, (cmap, cmulti))
+                sx, sy, cc_value = _cc_shift(R, vg, i, vol, parts_roi, roi, bufs, max_shift, multi, (cmap, cmulti))
                 shift = np.array([-sx, -sy], np.float32)  # the file holds the shift; the extra shift is its negation
                 if dump:
                     cc_maps.setdefault(i, []).append(cmap.cpu().numpy().copy())
@@ -355,17 +370,25 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
                 # the fitted model moves the particle's image by -s; the
                 # extra shift that moves it back is -s
                 shift = (-s).astype(np.float32)
-            # EmSartRefine.cpp:1024-1086: the group's shift to its particles
+            # EmSartRefine.cpp:1024-1086: the group's shift to its particles;
+            # the relations name the group (ByGroup) or the leader, and are
+            # kept for every receiver but a MaxCount / MaxDistance leader
             for g2 in receivers:
                 extra[i, g2] = shift
                 if mode != "ByGroup":
                     processed[g2] = True
+                if method == "cc" and (mode == "ByGroup" or g2 != lead):
+                    mm = motl[g2]
+                    relations[g2] = (int(mm[3]), int(mm[5]), int(mm[4]), group if mode == "ByGroup" else lead)
+                    rel_cc[g2] = cc_value
         for region, keep in reversed(saved):
             region.copy_(keep)
     if write:
         # the file holds the measured displacement (ShiftFile::SetValue);
         # EmSARTSubVolumes reads it negated as the extra shift
         F.write_shift_file(cfg.ShiftOutputFile, np.moveaxis(-extra, -1, 0))
+        if method == "cc":
+            write_relations(cfg.ShiftOutputFile + ".relations", relations, rel_cc)
         # one slice per group (EmSartRefine.cpp:986-1010)
         for i, maps in cc_maps.items():
             F.write_em(f"{cfg.CCMapFileName}{i}.em", np.stack(maps))

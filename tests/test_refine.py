@@ -308,6 +308,8 @@ def test_refine_cc_recovers_integer_shifts(tmp_path, multi):
     err = np.abs(got - es)
     assert err.max() <= 0.6 and err.mean() <= 0.35, (err, got, es)
     np.testing.assert_array_equal(F.read_shift_file(cfg.ShiftOutputFile), got)
+    # MaxCount leaders keep zeroed relations (only speed-up receivers get them)
+    assert (tmp_path / "shifts.em.relations").read_text() == "0; 0; 0; 0; 0\n" * 3
     S = cfg.MaxShift
     for i in range(es.shape[0]):
         maps, _ = F.read_em(str(tmp_path / f"ccmap_{i}.em"))
@@ -344,6 +346,13 @@ def test_refine_cc_groups(tmp_path, layout):
     np.testing.assert_array_equal(got[:, 0], got[:, 1])
     err = np.abs(got - es)
     assert err.max() <= 0.6 and err.mean() <= 0.35, (err, got, es)
+    # the relations file: particle number, group number, correlation maximum
+    lines = (tmp_path / "shifts.em.relations").read_text().splitlines()
+    assert len(lines) == es.shape[1]
+    fields = [ln.split("; ") for ln in lines]
+    assert [f[:4] for f in fields] == ([["1", "0", "0", "0"], ["2", "0", "0", "0"], ["3", "0", "0", "1"]]
+                                       if layout == "group" else [["1", "0", "0", "0"], ["2", "0", "0", "0"]])
+    assert all(0.0 < float(f[4]) <= 1.0 for f in fields)
 
 
 def _motl(coords, classes):
@@ -437,3 +446,11 @@ def test_group_iteration_and_speed_up():
     assert _visit(m, "MaxDistance", 0.0, max_distance=50.0) == [(g, [g]) for g in range(5)]
     assert _visit(m, "ByGroup", 0.0) == [(0, [0, 1]), (1, [2, 3]), (2, [4])]
     assert _visit(m, "MaxCount", 2.0, group_size=2, only=[2, 4]) == [(2, [3, 2]), (4, [4])]
+
+
+def test_relations_text_format(tmp_path):
+    from artiatomi_b200.refine import write_relations
+
+    rel = np.array([[12, 3, 7, 0], [0, 0, 0, 0], [5, 9, 1, 4]])
+    write_relations(str(tmp_path / "r"), rel, np.array([0.8125, 0.0, 1.0e-5], np.float32))
+    assert (tmp_path / "r").read_text() == "12; 3; 3; 0; 0.8125\n0; 0; 0; 0; 0\n5; 9; 9; 4; 1e-05\n"
