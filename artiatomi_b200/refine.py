@@ -383,6 +383,8 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
                     rel_cc[g2] = cc_value
         for region, keep in reversed(saved):
             region.copy_(keep)
+        if write:  # the shifts so far, in case the run stops (EmSartRefine.cpp:1091-1095)
+            F.write_shift_file(cfg.ShiftOutputFile, np.moveaxis(-extra, -1, 0))
     if write:
         # the file holds the measured displacement (ShiftFile::SetValue);
         # EmSARTSubVolumes reads it negated as the extra shift
