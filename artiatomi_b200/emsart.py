@@ -324,7 +324,8 @@ def sart_projection_update_noalloc(cfg: "ReconConfig", pg, vg, vol, real, sirt_c
     shared by all calls: overlapping calls on the GPU race, and the first call
     on a device, which looks up the array's address, should come before any
     stream capture. Same result as Reconstructor.reset_projections /
-    forward_projection / compare / back_projection.
+    forward_projection / compare / back_projection with the kernels that
+    cfg.variant names (FAITHFUL or FAST).
     """
     m = _f32(IDENTITY3 if mag is None else mag, 9)
     mi = _f32(IDENTITY3 if mag_inv is None else mag_inv, 9)

@@ -502,7 +502,13 @@ int esb_subvolume_wbp(esb_reconstructor* rec, const esb_vol_geom* full_vol, int 
  *    process exits. Projections larger than ESB_NOALLOC_MAX_PIXELS pixels are
  *    rejected with ESB_ERR_INVALID_ARGUMENT.
  *  - The first call on a device looks up the array's device address (set-up,
- *    once per device). Make that first call before any stream capture.
+ *    once per device and context; looked up again after a device reset
+ *    replaced the context). Make that first call before any stream capture.
+ *  - cfg->variant selects the kernels as on a reconstructor: FAITHFUL runs
+ *    the reference's arithmetic, FAST the closed-form projector and the
+ *    per-voxel-shadow back-projector (at the default launch shape: the
+ *    reconstructor's launch-shape trials need scratch buffers; the shape
+ *    does not change the result).
  *  - Every call shares the one array, and the array keeps the previous call's
  *    images; each call clears them first. Calls that overlap on the GPU (on
  *    different streams, or on different host threads, to the same device)
