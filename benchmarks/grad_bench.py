@@ -1,6 +1,6 @@
 """Differentiation workload: gradients of the projection loss and shift refinement.
 
-  python -m artiatomi_b200.grad_bench [--dims 512 512 128] [--proj 512] [--n-proj 41]
+  python -m benchmarks.grad_bench [--dims 512 512 128] [--proj 512] [--n-proj 41]
       [--max-shift 3] [--steps 20]
 
 Volume: a seeded ellipsoid phantom of the given size; 41 tilts (-60..+60
@@ -23,8 +23,8 @@ import numpy as np
 def main(argv=None):
     import torch
 
-    from . import emsart as E
-    from . import phantom as PH
+    from artiatomi_b200 import emsart as E
+    from artiatomi_b200 import phantom as PH
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--dims", type=int, nargs=3, default=[512, 512, 128])

@@ -1,6 +1,6 @@
 """Time single kernels of the hot path with CUDA events (for tuning and ncu).
 
-  python -m artiatomi_b200.kernel_bench --kernel fp|slicer|bp|bp_linear
+  python -m benchmarks.kernel_bench --kernel fp|slicer|bp|bp_linear
       [--dims X Y Z] [--proj W H] [--tilt DEG] [--os N] [--voxel f32|f16|bf16]
       [--reps R] [--warmup N] [--fast]
 
@@ -22,7 +22,7 @@ import numpy as np
 def main(argv=None):
     import torch
 
-    from . import emsart as E
+    from artiatomi_b200 import emsart as E
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="fp", choices=["fp", "slicer", "bp", "bp_linear", "travlen"])

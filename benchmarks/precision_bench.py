@@ -1,6 +1,6 @@
 """Volume storage precision: FP32, FP16 and BF16 SART with FP32 arithmetic.
 
-  python -m artiatomi_b200.precision_bench [--workload c5_precision] [--iterations 5]
+  python -m benchmarks.precision_bench [--workload c5_precision] [--iterations 5]
       [--no-graphs] [--crop-oracle]
 
 Runs the full SART + 3-D CTF reconstruction of the workload (default: the
@@ -28,7 +28,7 @@ DTYPES = ("f32", "f16", "bf16")
 def _run(wl, dtype, iterations, graphs):
     import torch
 
-    from . import emsart as E
+    from artiatomi_b200 import emsart as E
 
     td = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.bfloat16}[dtype]
     cfg = dataclasses.replace(wl.cfg, variant=E.VARIANT_FAST)
@@ -56,7 +56,7 @@ def _rel(a, b):
 def main(argv=None):
     import torch
 
-    from . import workloads as WL
+    from artiatomi_b200 import workloads as WL
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="c5_precision")
@@ -93,7 +93,7 @@ def crop_vs_oracle(iterations):
     from oracle import geometry as G
     from oracle.driver import OracleReconstructor
 
-    from . import workloads as WL
+    from artiatomi_b200 import workloads as WL
 
     wl = WL.build("c5_crop")
     tilt, xs, ys, psi = wl.markers

@@ -1,6 +1,6 @@
 """Throughput of EmSartRefine's shift measurement (method "cc").
 
-  python -m artiatomi_b200.refine_bench [--particles 16] [--dims 1024 1024 256]
+  python -m benchmarks.refine_bench [--particles 16] [--dims 1024 1024 256]
       [--proj 1024] [--n-proj 61] [--size 64] [--max-shift 10] [--no-ctf]
 
 One measurement is one particle in one projection, as EmSartRefine.cpp:
@@ -32,8 +32,8 @@ import numpy as np
 def main(argv=None):
     import torch
 
-    from . import emsart as E
-    from .refine import _cc_shift, _particle_roi, _remove_radius, _remove_subvolume
+    from artiatomi_b200 import emsart as E
+    from artiatomi_b200.refine import _cc_shift, _particle_roi, _remove_radius, _remove_subvolume
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--particles", type=int, default=16)

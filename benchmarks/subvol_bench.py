@@ -1,6 +1,6 @@
 """Batched against per-particle sub-volume weighted back-projection.
 
-  python -m artiatomi_b200.subvol_bench [--particles 2000] [--frame 4096 4096 1024]
+  python -m benchmarks.subvol_bench [--particles 2000] [--frame 4096 4096 1024]
       [--proj 4096] [--n-proj 61] [--os 2] [--no-ctf] [--warmup 1] [--reps 1]
 
 The sub-volume workload of EmSARTSubVolumes: particle centres uniform in the
@@ -60,8 +60,8 @@ def synthetic_projections(n, W, H, seed, n_ell=400):
 
 
 def build(particles, frame, W, H, n, os_, ctf, seed=0):
-    from . import _lib as L
-    from . import emsart as E
+    from artiatomi_b200 import _lib as L
+    from artiatomi_b200 import emsart as E
 
     rng = np.random.default_rng(seed)
     tilt = np.linspace(-60.0, 60.0, n).astype(np.float32)
@@ -90,7 +90,7 @@ def build(particles, frame, W, H, n, os_, ctf, seed=0):
 def main(argv=None):
     import torch
 
-    from . import emsart as E
+    from artiatomi_b200 import emsart as E
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--particles", type=int, default=2000)
