@@ -38,6 +38,13 @@ CONFIGS = {
     # 256^2, ellipsoid and bead counts scaled with the volume).
     "c5_crop": dict(dims=(256, 256, 64), W=256, H=256, n_proj=61, n_ell=40, n_beads=2, ctf=True, os=2, sirt=8,
                     lam=0.5, iterations=5, shift=2.0, psi=0.3, snr=0.1),
+    # The C2 geometry cropped to 256x256x64 (61 tilts of 256^2, the same
+    # angles, shifts, psi jitter, CTF, 30 nm slabs, oversampling 2, 4
+    # projections per subset, 2 iterations; ellipsoid and bead counts scaled
+    # with the volume): the size at which the FP32 and FP64 CPU oracles
+    # reconstruct the C2 parameters in minutes.
+    "c2_crop": dict(dims=(256, 256, 64), W=256, H=256, n_proj=61, n_ell=78, n_beads=5, ctf=True, os=2, sirt=4,
+                    lam=0.5, iterations=2, shift=2.0, psi=0.3, snr=0.1),
     "c2_sart_ctf_z64": dict(dims=(1024, 1024, 64), W=1024, H=1024, n_proj=61, n_ell=1250, n_beads=75, ctf=True, os=2,
                             sirt=4, lam=0.5, iterations=2, shift=2.0, psi=0.3, snr=0.1),
 }

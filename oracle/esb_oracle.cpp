@@ -358,7 +358,14 @@ inline float taper(float w) {
 // One 4-voxel quad of kernel `backProjection` / `backProjectionFP16`
 // (BackProjectionSquareOS.cu:263-782, 786-1291).  Returns false when the
 // quad's first corner lies outside [distMin, distMax) (slab test :365-369).
-template <class R>
+//
+// R is the arithmetic of the chords and sums, D that of the decisions: the
+// quad's depth against the slab bounds and the macro-cell rectangle whose
+// integer bounds pick the samples. R = D = float is the reference; R = D =
+// double its FP64 evaluation; R = double, D = float keeps the reference's
+// float decisions with exact chords (what the library's FAST kernels
+// compute), to attribute differences between the two.
+template <class R, class D>
 void bp_quad(const OrcGeom& g, void* volData, int dtype, int qx, int y, int z, const float* img, int pw,
              int ph, size_t pitchElems, float lambda, int os, float distMin, float distMax, bool linear,
              bool q9) {
@@ -373,39 +380,43 @@ void bp_quad(const OrcGeom& g, void* volData, int dtype, int qx, int y, int z, c
     else vb[k] = bf16_to_float(((uint16_t*)volData)[base + k]);
   }
   const int x = 4 * qx;
-  R bbMin[3] = {R(g.bbMin[0]), R(g.bbMin[1]), R(g.bbMin[2])};
-  R vs[3] = {R(g.vs[0]), R(g.vs[1]), R(g.vs[2])};
-  R n[3] = {R(g.n[0]), R(g.n[1]), R(g.n[2])};
-  R det[3] = {R(g.det[0]), R(g.det[1]), R(g.det[2])};
-  R mcMin[3] = {bbMin[0] + R(x) * vs[0], bbMin[1] + R(y) * vs[1], bbMin[2] + R(z) * vs[2]};
-  R mcMax[3] = {bbMin[0] + R(x + 5) * vs[0], bbMin[1] + R(y + 1) * vs[1], bbMin[2] + R(z + 1) * vs[2]};
-  R ndet = -n[0] * det[0] - n[1] * det[1] - n[2] * det[2];
-  R bmin[3] = {R(FLT_MAX), R(FLT_MAX), R(FLT_MAX)};
-  R bmax[3] = {R(-200000.f), R(-200000.f), R(-200000.f)};
+  const D dbbMin[3] = {D(g.bbMin[0]), D(g.bbMin[1]), D(g.bbMin[2])};
+  const D dvs[3] = {D(g.vs[0]), D(g.vs[1]), D(g.vs[2])};
+  const D dn[3] = {D(g.n[0]), D(g.n[1]), D(g.n[2])};
+  const D ddet[3] = {D(g.det[0]), D(g.det[1]), D(g.det[2])};
+  D mcMin[3] = {dbbMin[0] + D(x) * dvs[0], dbbMin[1] + D(y) * dvs[1], dbbMin[2] + D(z) * dvs[2]};
+  D mcMax[3] = {dbbMin[0] + D(x + 5) * dvs[0], dbbMin[1] + D(y + 1) * dvs[1], dbbMin[2] + D(z + 1) * dvs[2]};
+  D ndet = -dn[0] * ddet[0] - dn[1] * ddet[1] - dn[2] * ddet[2];
+  D bmin[3] = {D(FLT_MAX), D(FLT_MAX), D(FLT_MAX)};
+  D bmax[3] = {D(-200000.f), D(-200000.f), D(-200000.f)};
   for (int c = 0; c < 8; ++c) {
     // corner order of the unrolled loop: (x, y, z) bits = (c>>2, c>>1, c)&1
-    R p[3] = {(c & 4) ? mcMin[0] + (mcMax[0] - mcMin[0]) : mcMin[0],
+    D p[3] = {(c & 4) ? mcMin[0] + (mcMax[0] - mcMin[0]) : mcMin[0],
               (c & 2) ? mcMin[1] + (mcMax[1] - mcMin[1]) : mcMin[1],
               (c & 1) ? mcMin[2] + (mcMax[2] - mcMin[2]) : mcMin[2]};
-    R t = (n[0] * p[0] + n[1] * p[1] + n[2] * p[2]);
+    D t = (dn[0] * p[0] + dn[1] * p[1] + dn[2] * p[2]);
     t += ndet;
     t = std::fabs(t);
-    if (c == 0 && !(t >= R(distMin) && t < R(distMax))) return;
+    if (c == 0 && !(t >= D(distMin) && t < D(distMax))) return;
     for (int k = 0; k < 3; ++k) {
-      R hp = t * (-n[k]) + p[k];
+      D hp = t * (-dn[k]) + p[k];
       bmin[k] = fmn(hp, bmin[k]);
       bmax[k] = fmx(hp, bmax[k]);
     }
   }
-  R lo[3], hi[3];
+  D lo[3], hi[3];
   for (int k = 0; k < 3; ++k) { lo[k] = fmn(bmin[k], bmax[k]); hi[k] = fmx(bmin[k], bmax[k]); }
-  if (n[0] <= R(0)) std::swap(lo[0], hi[0]);
-  auto detmul = [&](const R p[3], R o[3]) {
+  if (dn[0] <= D(0)) std::swap(lo[0], hi[0]);
+  auto detmul = [&](const D p[3], D o[3]) {
     for (int r = 0; r < 3; ++r)
-      o[r] = R(g.detMat[r * 4 + 0]) * p[0] + R(g.detMat[r * 4 + 1]) * p[1] + R(g.detMat[r * 4 + 2]) * p[2] +
-             R(1) * R(g.detMat[r * 4 + 3]);
+      o[r] = D(g.detMat[r * 4 + 0]) * p[0] + D(g.detMat[r * 4 + 1]) * p[1] + D(g.detMat[r * 4 + 2]) * p[2] +
+             D(1) * D(g.detMat[r * 4 + 3]);
   };
-  R plo[3], phi[3];
+  R bbMin[3] = {R(g.bbMin[0]), R(g.bbMin[1]), R(g.bbMin[2])};
+  R vs[3] = {R(g.vs[0]), R(g.vs[1]), R(g.vs[2])};
+  R n[3] = {R(g.n[0]), R(g.n[1]), R(g.n[2])};
+  R det[3] = {R(g.det[0]), R(g.det[1]), R(g.det[2])};
+  D plo[3], phi[3];
   detmul(lo, plo);
   detmul(hi, phi);
   int pb_x = (int)std::floor(fmn(plo[0], phi[0]));
@@ -690,10 +701,15 @@ int orc_bp(const OrcGeom* g, void* vol, int dtype, const float* img, int proj_x,
   parallel_for(nz * ny, nthreads, [&](int zy) {
     int z = zy / ny, y = zy % ny;
     for (int q = 0; q < nq; ++q) {
-      if (precision)
-        bp_quad<double>(*g, vol, dtype, q, y, z, img, proj_x, proj_y, proj_x, lambda, os, distMin, distMax, linear, q9);
+      if (precision == 2)  // float decisions, double chords and sums
+        bp_quad<double, float>(*g, vol, dtype, q, y, z, img, proj_x, proj_y, proj_x, lambda, os, distMin, distMax,
+                               linear, q9);
+      else if (precision)
+        bp_quad<double, double>(*g, vol, dtype, q, y, z, img, proj_x, proj_y, proj_x, lambda, os, distMin, distMax,
+                                linear, q9);
       else
-        bp_quad<float>(*g, vol, dtype, q, y, z, img, proj_x, proj_y, proj_x, lambda, os, distMin, distMax, linear, q9);
+        bp_quad<float, float>(*g, vol, dtype, q, y, z, img, proj_x, proj_y, proj_x, lambda, os, distMin, distMax,
+                              linear, q9);
     }
   });
   return 0;
