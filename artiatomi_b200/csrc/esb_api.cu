@@ -37,9 +37,9 @@ cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img,
 cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
                                  const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
                                  float distMin, float distMax, int linear, cudaStream_t st, int transposed,
-                                 const float* ups = nullptr, size_t up_stride = 0, const BpShape* shape = nullptr);
-cudaError_t launch_upsample(const float* imgs, size_t img_stride, int count, int pw, int ph, int os, int linear,
-                            float* up, size_t up_stride, cudaStream_t st);
+                                 const float2* ups = nullptr, size_t up_stride = 0, const BpShape* shape = nullptr);
+cudaError_t launch_upsample(const KConst& k, const float* imgs, size_t img_stride, int count, int pw, int ph, int os,
+                            int linear, float2* up, size_t up_stride, cudaStream_t st);
 bool bp_can_upsample(const KConst& k, int os);
 bool bp_uses_axis(const KConst& k, int os);
 cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float* imgs, size_t img_stride,
@@ -440,7 +440,7 @@ struct esb_reconstructor {
   PhaseTimer timers[4];
   float* slab_imgs = nullptr;  // per-slab images of the fused CTF paths
   size_t slab_cap = 0;         // capacity in images
-  float* up_imgs = nullptr;    // the slab images pre-sampled on the sub-pixel grid
+  float2* up_imgs = nullptr;   // the slab images pre-sampled on the sub-pixel grid, with sample rows
   size_t up_cap = 0;           // capacity in floats
   void* tune_scratch = nullptr;  // the autotuner's trial outputs
   size_t tune_cap = 0;           // capacity in bytes
@@ -844,7 +844,7 @@ static int rec_march_nw(esb_reconstructor* r, const KConst& c, const void* vol, 
 // Block shape of the single-axis back-projection for this problem; trials on
 // a scratch slab of up to 32 planes from the middle of the volume.
 static BpShape rec_bp_shape(esb_reconstructor* r, const KConst& c, int vt, const float* imgs, size_t img_stride,
-                            const SlabTable& T, int linear, const float* up, size_t up_stride) {
+                            const SlabTable& T, int linear, const float2* up, size_t up_stride) {
   const int W = r->cfg.proj_x, H = r->cfg.proj_y, os = r->cfg.oversampling;
   BpShape s{kBpShapes[0][0], kBpShapes[0][1], 0, 0};
   if (!bp_uses_axis(c, os)) return s;
@@ -1069,28 +1069,28 @@ static int rec_subvol_slab_images(esb_reconstructor* r, const esb_vol_geom* full
 // Pre-samples `count` transposed slab images for the back-projection
 // (launch_upsample); returns NULL when the geometry does not allow it
 // (oversampling not a power of two, magnification anisotropy) or the
-// images would exceed 4 GiB, and the back-projection then filters the slab
-// images itself. `up_stride` receives the floats per pre-sampled image.
-static const float* rec_upsample(esb_reconstructor* r, const KConst& c, int count, int linear, size_t& up_stride) {
+// images would exceed 8 GiB, and the back-projection then filters the slab
+// images itself. `up_stride` receives the (value, row) pairs per image.
+static const float2* rec_upsample(esb_reconstructor* r, const KConst& c, int count, int linear, size_t& up_stride) {
   const esb_recon_config& cf = r->cfg;
   const int os = cf.oversampling;
   up_stride = (size_t)cf.proj_x * os * (size_t)cf.proj_y * os;
   const size_t need = up_stride * (size_t)count;
-  if (!bp_can_upsample(c, os) || need * sizeof(float) > ((size_t)4 << 30)) return nullptr;
+  if (!bp_can_upsample(c, os) || need * sizeof(float2) > ((size_t)8 << 30)) return nullptr;
   if (need > r->up_cap) {
     if (cudaStreamSynchronize(r->stream) != cudaSuccess) return nullptr;
     cudaFree(r->up_imgs);
     r->up_imgs = nullptr;
     r->up_cap = 0;
-    if (cudaMalloc(&r->up_imgs, need * sizeof(float)) != cudaSuccess) {
+    if (cudaMalloc(&r->up_imgs, need * sizeof(float2)) != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
     r->up_cap = need;
   }
   const size_t img = (size_t)cf.proj_x * cf.proj_y;
-  if (launch_upsample(r->slab_imgs, img, count, cf.proj_x, cf.proj_y, os, linear, r->up_imgs, up_stride, r->stream) !=
-      cudaSuccess)
+  if (launch_upsample(c, r->slab_imgs, img, count, cf.proj_x, cf.proj_y, os, linear, r->up_imgs, up_stride,
+                      r->stream) != cudaSuccess)
     return nullptr;
   return r->up_imgs;
 }
@@ -1234,7 +1234,7 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
       none.count = 0;
       PhaseScope ps(r, 1);
       size_t up_stride = 0;
-      const float* up = rec_upsample(r, c, 1, 0, up_stride);
+      const float2* up = rec_upsample(r, c, 1, 0, up_stride);
       ESB_CK(cudaGetLastError(), "back projection");
       const BpShape shape = rec_bp_shape(r, c, voxel_type, r->slab_imgs, 0, none, 0, up, up_stride);
       ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, 0, none, W, H, W, lambda, cf.oversampling, 0.0f,
@@ -1259,7 +1259,7 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
     if ((rc = rec_ctf_chain_slabs(r, T, index, img, 1, 1, p, 0, r->slab_imgs, nullptr, 1, p, 1))) return rc;
     PhaseScope ps(r, 1);
     size_t up_stride = 0;
-    const float* up = rec_upsample(r, c, T.count, 1, up_stride);
+    const float2* up = rec_upsample(r, c, T.count, 1, up_stride);
     ESB_CK(cudaGetLastError(), "back projection");
     const BpShape shape = rec_bp_shape(r, c, voxel_type, r->slab_imgs, (size_t)W * H, T, 1, up, up_stride);
     ESB_CK(launch_bp_fast_slabs(c, vol, voxel_type, r->slab_imgs, (size_t)W * H, T, W, H, W, lambda, cf.oversampling,

@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __res
                                                  const float* __restrict__ imgs, size_t img_stride, SlabTable slabs,
                                                  int pw, int ph, size_t pitchE, float lambda, int os, float inv,
                                                  float distMin, float distMax, int linear, int transposed,
-                                                 const float* __restrict__ ups, size_t up_stride) {
+                                                 const float2* __restrict__ ups, size_t up_stride) {
   const int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int z = (int)blockIdx.z;
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128) k_bp_fast(KConst k, BpGeom g, void* __res
   int pbx, pby, pbz, pbw;
   macro_footprint(k, x, y, z, pw, ph, depth, pbx, pby, pbz, pbw);
   const float* img = imgs;
-  const float* up = ups;
+  const float2* up = ups;
   if (slabs.count > 0) {  // fused CTF slabs
     if (!(depth >= slabs.bound[0] && depth < slabs.bound[slabs.count])) return;
     int s = 0;
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
                                                  const float* __restrict__ imgs, size_t img_stride, SlabTable slabs,
                                                  int pw, int ph, size_t pitchE, float lambda, int os, float inv,
                                                  float distMin, float distMax, int linear, int transposed,
-                                                 const float* __restrict__ ups, size_t up_stride, int z0) {
+                                                 const float2* __restrict__ ups, size_t up_stride, int z0) {
   // plane z0 + blockIdx.z of the geometry, stored at plane blockIdx.z of vol
   // (z0 = 0 but for the autotuner's trial launches on a scratch slab)
   const int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
   const int x = 4 * q;
   const float depth = macro_depth(k, x, y, z);
   const float* img = imgs;
-  const float* up = ups;
+  const float2* up = ups;
   if (slabs.count > 0) {
     if (!(depth >= slabs.bound[0] && depth < slabs.bound[slabs.count])) return;
     int s = 0;
@@ -120,26 +120,38 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
   const float fos = (float)os;
   const float cy = k.bbMin.y + ((float)y + 0.5f) * k.vs.y, cz = k.bbMin.z + ((float)z + 0.5f) * k.vs.z;
   const float uyz = g.U.y * cy + g.U.z * cz + g.U0, vyz = g.V.y * cy + g.V.z * cz + g.V0;
-  const float dwv = inv * g.wv, dyv = inv * g.yv;
+  const float dwv = inv * g.wv;
   const bool lin = linear != 0, tr = transposed != 0;
   const bool interior = !lin || (pbx >= 1 && pbz >= 1);
   const size_t sx = tr ? (size_t)ph : 1, sy = tr ? 1 : pitchE;
-  auto read = [&](int mu, int mv) -> float {
-    if (UP) return __ldg(up + (size_t)mu * upH + mv);
-    const float px = ((float)mu + 0.5f) * inv, py = ((float)mv + 0.5f) * inv;
-    return interior ? sample_interior(img, sx, sy, px, py, lin) : sample_image(img, pw, ph, pitchE, px, py, lin, tr);
-  };
   const long base = ((long)zl * ny + y) * (long)k.dim.x + x;
   float res[4], has[4];
-  const bool patch = !UP && os == 2 && lin && interior;
+  if (UP) {
+    auto read = [&](int mu, int mv) -> float2 { return __ldg(up + (size_t)mu * upH + mv); };
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float cx = k.bbMin.x + ((float)(x + i) + 0.5f) * k.vs.x;
-    const float uc = g.U.x * cx + uyz, vc = g.V.x * cx + vyz;
-    if (!(patch && axis_sums_os2(g, uc, vc, dwv, dyv, pbx * 2, pby * 2 - 1, pbz * 2, pbw * 2 - 1, img, sx, sy, pw, ph,
-                                 res[i], has[i])))
-      axis_sums<!UP>(g, uc, vc, fos, inv, dwv, dyv, pbx * os, pby * os - 1, pbz * os, pbw * os - 1, read, res[i],
+    for (int i = 0; i < 4; ++i) {
+      const float cx = k.bbMin.x + ((float)(x + i) + 0.5f) * k.vs.x;
+      const float uc = g.U.x * cx + uyz, vc = g.V.x * cx + vyz;
+      axis_sums_rows(g, uc, vc, fos, inv, dwv, y, pbx * os, pby * os - 1, pbz * os, pbw * os - 1, read, res[i],
                      has[i]);
+    }
+  } else {
+    auto read = [&](int mu, int mv) -> float {
+      const float px = ((float)mu + 0.5f) * inv, py = ((float)mv + 0.5f) * inv;
+      return interior ? sample_interior(img, sx, sy, px, py, lin) : sample_image(img, pw, ph, pitchE, px, py, lin, tr);
+    };
+    const bool patch = os == 2 && lin && interior;
+    const float cx0 = k.bbMin.x + ((float)x + 0.5f) * k.vs.x;
+    const RowAnchor anchor(g, y, g.U.x * cx0 + uyz, g.V.x * cx0 + vyz, fos);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float cx = k.bbMin.x + ((float)(x + i) + 0.5f) * k.vs.x;
+      const float uc = g.U.x * cx + uyz, vc = g.V.x * cx + vyz;
+      if (!(patch && axis_sums_os2(g, uc, vc, dwv, anchor, pbx * 2, pby * 2 - 1, pbz * 2, pbw * 2 - 1, img, sx, sy,
+                                   pw, ph, res[i], has[i])))
+        axis_sums(g, uc, vc, fos, inv, dwv, anchor, pbx * os, pby * os - 1, pbz * os, pbw * os - 1, read, res[i],
+                  has[i]);
+    }
   }
   if (VT == ESB_VOXEL_F32 && (((uintptr_t)((float*)vol + base)) & 15) == 0) {
     float4 v = *((float4*)((float*)vol + base));
@@ -158,11 +170,12 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
 }
 
 // The slab images (transposed, [x][y], stride img_stride) sampled at every
-// sub-pixel grid point: up[s][mu][mv] = image s at ((mu + 0.5) / os,
-// (mv + 0.5) / os), clamp addressing, nearest or bilinear as the
-// back-projection reads it.
+// sub-pixel grid point, with the voxel row of the grid point's ray:
+// up[s][mu][mv] = (image s at ((mu + 0.5) / os, (mv + 0.5) / os), row as int
+// bits), clamp addressing, nearest or bilinear as the back-projection reads
+// it (sample_row; meaningful for single-axis projections, which read it).
 __global__ void __launch_bounds__(256) k_upsample(const float* __restrict__ imgs, size_t img_stride, int pw, int ph,
-                                                  int os, float inv, int linear, float* __restrict__ up,
+                                                  int os, float inv, int linear, RowGeom rg, float2* __restrict__ up,
                                                   size_t up_stride) {
   const int mv = blockIdx.x * blockDim.x + threadIdx.x;
   const int mu = blockIdx.y;
@@ -171,7 +184,8 @@ __global__ void __launch_bounds__(256) k_upsample(const float* __restrict__ imgs
   if (mv >= upH) return;
   const float px = ((float)mu + 0.5f) * inv, py = ((float)mv + 0.5f) * inv;
   up[(size_t)s * up_stride + (size_t)mu * upH + mv] =
-      sample_image(imgs + (size_t)s * img_stride, pw, ph, (size_t)pw, px, py, linear != 0, true);
+      make_float2(sample_image(imgs + (size_t)s * img_stride, pw, ph, (size_t)pw, px, py, linear != 0, true),
+                  __int_as_float(sample_row(rg, mu, mv)));
 }
 
 }  // namespace
@@ -179,7 +193,7 @@ __global__ void __launch_bounds__(256) k_upsample(const float* __restrict__ imgs
 cudaError_t launch_bp_fast_slabs(const KConst& k, void* vol, int vt, const float* imgs, size_t img_stride,
                                  const SlabTable& slabs, int pw, int ph, size_t pitchE, float lambda, int os,
                                  float distMin, float distMax, int linear, cudaStream_t st, int transposed,
-                                 const float* ups, size_t up_stride, const BpShape* shape) {
+                                 const float2* ups, size_t up_stride, const BpShape* shape) {
   const int nq = k.dimXQuarter, ny = (int)k.dim.y, nz = (int)k.dim.z;
   if (nq <= 0 || ny <= 0 || nz <= 0) return cudaSuccess;
   const BpGeom g = make_geom(k, os);
@@ -226,13 +240,15 @@ cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img,
                               nullptr, 0, nullptr);
 }
 
-// Pre-sampled slab images for k_bp_fast (transposed input images, up_stride
-// floats per output image of (pw * os) x (ph * os)).
-cudaError_t launch_upsample(const float* imgs, size_t img_stride, int count, int pw, int ph, int os, int linear,
-                            float* up, size_t up_stride, cudaStream_t st) {
+// Pre-sampled slab images for k_bp_fast / k_bp_axis (transposed input
+// images, up_stride (value, row) pairs per output image of (pw * os) x
+// (ph * os)); k gives the geometry of the rows.
+cudaError_t launch_upsample(const KConst& k, const float* imgs, size_t img_stride, int count, int pw, int ph, int os,
+                            int linear, float2* up, size_t up_stride, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   dim3 blk(256), grd((ph * os + 255) / 256, pw * os, count);
-  k_upsample<<<grd, blk, 0, st>>>(imgs, img_stride, pw, ph, os, 1.0f / (float)os, linear, up, up_stride);
+  k_upsample<<<grd, blk, 0, st>>>(imgs, img_stride, pw, ph, os, 1.0f / (float)os, linear, make_row_geom(k, os), up,
+                                  up_stride);
   ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }

@@ -156,7 +156,7 @@ __device__ __forceinline__ float sample_interior(const float* __restrict__ img, 
 __device__ __forceinline__ void voxel_sums(const KConst& k, const BpGeom& g, const float* __restrict__ img, int pw,
                                            int ph, size_t pitchE, int os, float inv, bool linear, bool transposed,
                                            int x, int y, int z, int pbx, int pby, int pbz, int pbw, float& acc,
-                                           float& dacc, const float* __restrict__ up = nullptr, int upH = 0) {
+                                           float& dacc, const float2* __restrict__ up = nullptr, int upH = 0) {
   const float cx = k.bbMin.x + ((float)x + 0.5f) * k.vs.x, cy = k.bbMin.y + ((float)y + 0.5f) * k.vs.y,
               cz = k.bbMin.z + ((float)z + 0.5f) * k.vs.z;
   const float uc = g.U.x * cx + g.U.y * cy + g.U.z * cz + g.U0;
@@ -177,12 +177,12 @@ __device__ __forceinline__ void voxel_sums(const KConst& k, const BpGeom& g, con
     for (float py = py0; py < (float)pbw && py <= vb; py = fadd(py, inv)) {
       const float dv = py - vc;
       float dx = du0 * g.u.x + dv * g.v.x, dy = du0 * g.u.y + dv * g.v.y, dz = du0 * g.u.z + dv * g.v.z;
-      const float* p = up + mu0 * (size_t)upH + (size_t)(int)(py * fos - 0.5f);
+      const float2* p = up + mu0 * (size_t)upH + (size_t)(int)(py * fos - 0.5f);
 #pragma unroll 1
       for (float px = px0; px < (float)pby && px <= ub; px = fadd(px, inv)) {
         const float L = chord(dx, dy, dz, g);
         if (L > 0.0f) {
-          a += __ldg(p) * L;
+          a += __ldg(p).x * L;
           da += L;
         }
         dx += ix;
@@ -248,6 +248,89 @@ inline BpGeom make_geom(const KConst& k, int os) {
   return g;
 }
 
+// Voxel row of a sample's ray in a single-axis projection. With n.y = 0 a
+// ray runs parallel to the voxels' y faces, so it passes through a voxel
+// row fully or not at all: the row test is a step. Where the sub-pixel
+// sample grid lines up with the voxel grid (the in-plane rotation of the
+// tilt axis makes some detector region do so on every projection) rays
+// graze the faces within ~1e-5 of a voxel, and an offset taken from a
+// voxel centre's float detector coordinate decides them at random. The
+// test is therefore made from the world y of the ray of sample (mu, mv) at
+// the volume's centre depth, Y = ry0 + mu u + mv v with u = u_pitch.y / os
+// and v = v_pitch.y / os (exact floats for power-of-two os), taken relative
+// to a voxel row without rounding error in its large terms (row_offset).
+// A is ry0 - bbMin.y - vs / 2 as an unevaluated float pair (A + Al).
+struct RowGeom {
+  float A, Al;
+  float u, v;  // Y per sample along the detector's u and v axes
+  float vs;    // voxel size in y
+  int ny;      // voxel rows
+};
+
+inline RowGeom make_row_geom(const KConst& k, int os) {
+  RowGeom r;
+  double t0 = 0.0;  // depth of the volume's centre along n from the detector plane
+  const double nn[3] = {k.n.x, k.n.y, k.n.z}, dd[3] = {k.det.x, k.det.y, k.det.z};
+  const double lo[3] = {k.bbMin.x, k.bbMin.y, k.bbMin.z}, hv[3] = {k.vs.x, k.vs.y, k.vs.z};
+  const double nd[3] = {k.dim.x, k.dim.y, k.dim.z};
+  for (int j = 0; j < 3; ++j) t0 += nn[j] * (lo[j] + 0.5 * hv[j] * nd[j] - dd[j]);
+  r.u = k.u.y / (float)os;
+  r.v = k.v.y / (float)os;
+  const double ry0 = (double)k.det.y + t0 * (double)k.n.y + 0.5 * ((double)r.u + (double)r.v);
+  const double A = ry0 - (double)k.bbMin.y - 0.5 * (double)k.vs.y;
+  r.A = (float)A;
+  r.Al = (float)(A - (double)r.A);
+  r.vs = k.vs.y;
+  r.ny = (int)k.dim.y;
+  return r;
+}
+
+// Error-free transformations (Knuth's two-sum, and the product's rounding
+// error from a fused multiply-add): s + e == a + b and p + e == a * b
+// exactly.
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+__device__ __forceinline__ void two_prod(float a, float b, float& p, float& e) {
+  p = __fmul_rn(a, b);
+  e = __fmaf_rn(a, b, -p);
+}
+
+// Offset of the ray of sample (mu, mv) from the centre plane of voxel row
+// yrow: A + mu u + mv v - yrow vs. The terms are hundreds of voxels while
+// the sum near a voxel is below about a voxel, so it is formed without
+// rounding error in the large terms; the result is exact to its own float
+// rounding.
+__device__ __forceinline__ float row_offset(const RowGeom& r, int yrow, int mu, int mv) {
+  float p1, e1, p2, e2, p3, e3, s1, t1, s2, t2, s3, t3;
+  two_prod((float)mu, r.u, p1, e1);
+  two_prod((float)mv, r.v, p2, e2);
+  two_prod(-(float)yrow, r.vs, p3, e3);
+  two_sum(r.A, p1, s1, t1);
+  two_sum(s1, p3, s2, t2);
+  two_sum(s2, p2, s3, t3);
+  return __fadd_rn(s3, __fadd_rn(__fadd_rn(__fadd_rn(r.Al, e1), __fadd_rn(e2, e3)), __fadd_rn(t1, __fadd_rn(t2, t3))));
+}
+
+// Voxel row whose interior holds the ray of sample (mu, mv), or -1 (a ray on
+// a face, or outside the volume): the reference's slab test evaluated
+// exactly, which counts a ray strictly inside the row.
+__device__ __forceinline__ int sample_row(const RowGeom& r, int mu, int mv) {
+  const float h = 0.5f * r.vs;
+  int y = (int)floorf(row_offset(r, 0, mu, mv) / r.vs + 0.5f);  // within a row of the answer
+  float o = row_offset(r, y, mu, mv);
+  if (o >= h) {
+    ++y;
+    o = row_offset(r, y, mu, mv);
+  } else if (o <= -h) {
+    --y;
+    o = row_offset(r, y, mu, mv);
+  }
+  return (fabsf(o) < h && y >= 0 && y < r.ny) ? y : -1;
+}
+
 // Geometry of the single-axis back-projection (axis_sums): tilt axis along
 // y (n.y = 0), power-of-two oversampling, no magnification anisotropy.
 struct AxisGeom {
@@ -257,6 +340,7 @@ struct AxisGeom {
   float wu, wv;    // in-plane offset of a sample perpendicular to n in x-z, per pixel of u and v
   float yu, yv;    // its y component per pixel of u and v
   float hby;       // half voxel size in y
+  RowGeom r;       // the row test of a sample's ray (RowGeom)
   float L0, w1K, K;  // chord trapezoid: L(w) = min(L0, max(0, w1K - |w| K))
   // macro-cell rectangle of quad (x, y, z), affine in the quad position:
   // u_lo/hi = ru.w + x ru.x + y ru.y + z ru.z + (ulo, uhi), same for v
@@ -316,6 +400,7 @@ inline AxisGeom make_axis_geom(const KConst& k, const BpGeom& b, int os) {
   g.yu = k.u.y;
   g.yv = k.v.y;
   g.hby = b.hb.y;
+  g.r = make_row_geom(k, os);
   const float anx = fabsf(k.n.x), anz = fabsf(k.n.z);
   const float hx = b.hb.x, hz = b.hb.z;
   g.L0 = fminf(anx > 0.f ? 2.f * hx / anx : FLT_MAX, anz > 0.f ? 2.f * hz / anz : FLT_MAX);
@@ -398,23 +483,75 @@ inline bool axis_eligible(const KConst& k, const BpGeom& g) {
   return g.exact_grid && g.aniso_identity && fabsf(k.n.y) <= 1e-6f;
 }
 
-// sum(sample*chord) and sum(chord) of one voxel whose centre projects to
-// (uc, vc), for a single-axis projection. With n.y = 0 the chord of a
-// sample's ray through the voxel depends only on the ray's offset w from the
-// voxel centre perpendicular to n in the x-z plane (a trapezoid: the plateau
-// min(2 hx / |n.x|, 2 hz / |n.z|), falling linearly to 0 at
-// |w| = hx |n.z| + hz |n.x| with slope 1 / (|n.x| |n.z|)), cut to 0 where the
-// offset's y component leaves the voxel. Samples are the sub-pixel grid
-// points (m + 0.5) / os inside the voxel's shadow and inside
-// [mu_min, mu_max] x [mv_min, mv_max] (the quad's macro-cell rectangle);
-// read(mu, mv) returns the image at grid point (mu, mv). SKIP (filtered
-// 4-texel reads): loops with a branch that reads only samples with a
-// nonzero chord; otherwise (one load per sample, pre-sampled images) the
-// first 2 x 3 samples are unrolled and read unconditionally.
-template <bool SKIP, class Read>
+// row_offset of the samples of the voxels of one row (the 4 voxels of a
+// quad): formed once, at sample (mu, mv) near the first voxel's centre
+// projection (|y| below about a voxel), and stepped from there in float by
+// the few sample positions to each voxel's first sample, which keeps the
+// value exact to float rounding of a sub-voxel offset.
+struct RowAnchor {
+  int mu, mv;
+  float y;
+  __device__ __forceinline__ RowAnchor(const AxisGeom& g, int yrow, float uc, float vc, float fos)
+      : mu((int)floorf(uc * fos)), mv((int)floorf(vc * fos)) {
+    y = row_offset(g.r, yrow, mu, mv);
+  }
+  __device__ __forceinline__ float at(const AxisGeom& g, int mu_, int mv_) const {
+    return fmaf((float)(mv_ - mv), g.r.v, fmaf((float)(mu_ - mu), g.r.u, y));
+  }
+};
+
+// sum(sample*chord) and sum(chord) of one voxel (of the row of `anchor`)
+// whose centre projects to (uc, vc), for a single-axis projection. With
+// n.y = 0 the chord of a sample's ray through the voxel depends only on the
+// ray's offset w from the voxel centre perpendicular to n in the x-z plane
+// (a trapezoid: the plateau min(2 hx / |n.x|, 2 hz / |n.z|), falling
+// linearly to 0 at |w| = hx |n.z| + hz |n.x| with slope 1 / (|n.x| |n.z|)),
+// and is 0 where the ray lies outside the voxel row (RowGeom). Samples are
+// the sub-pixel grid points (m + 0.5) / os inside the voxel's shadow and
+// inside [mu_min, mu_max] x [mv_min, mv_max] (the quad's macro-cell
+// rectangle); read(mu, mv) returns the image at grid point (mu, mv), a
+// filtered read taken only for samples with a nonzero chord.
+template <class Read>
 __device__ __forceinline__ void axis_sums(const AxisGeom& g, float uc, float vc, float fos, float inv, float dwv,
-                                          float dyv, int mu_min, int mu_max, int mv_min, int mv_max, const Read& read,
-                                          float& acc, float& dacc) {
+                                          const RowAnchor& anchor, int mu_min, int mu_max, int mv_min, int mv_max,
+                                          const Read& read, float& acc, float& dacc) {
+  const int mu0 = max((int)ceilf((uc - g.hu) * fos - 0.5f), mu_min);
+  const int mu1 = min((int)floorf((uc + g.hu) * fos - 0.5f), mu_max);
+  const int mv0 = max((int)ceilf((vc - g.hv) * fos - 0.5f), mv_min);
+  const int mv1 = min((int)floorf((vc + g.hv) * fos - 0.5f), mv_max);
+  const float dv0 = ((float)mv0 + 0.5f) * inv - vc;
+  float a = 0.f, da = 0.f;
+  const int rows = mu1 - mu0 + 1;
+  const int cnt = mv1 - mv0 + 1;
+  const float y00 = anchor.at(g, mu0, mv0);
+#pragma unroll 1
+  for (int r = 0; r < rows; ++r) {
+    const int mu = mu0 + r;
+    const float du = ((float)mu + 0.5f) * inv - uc;
+    const float w = du * g.wu + dv0 * g.wv, dy = fmaf((float)r, g.r.u, y00);
+#pragma unroll 1
+    for (int j = 0; j < cnt; ++j) {
+      const float ww = fmaf((float)j, dwv, w), yy = fmaf((float)j, g.r.v, dy);
+      const float L = fminf(g.L0, fmaxf(0.f, fmaf(-fabsf(ww), g.K, g.w1K)));
+      if (fabsf(yy) < g.hby && L > 0.f) {
+        a = fmaf(read(mu, mv0 + j), L, a);
+        da += L;
+      }
+    }
+  }
+  acc = a;
+  dacc = da;
+}
+
+// axis_sums on images pre-sampled with the voxel row of every sample's ray
+// (k_upsample): read(mu, mv) returns (value, row as int bits), and a sample
+// counts for voxel row yrow when its row is yrow. One 8-byte load per sample;
+// the first 2 x 3 samples of a voxel's shadow are unrolled and read
+// unconditionally.
+template <class Read>
+__device__ __forceinline__ void axis_sums_rows(const AxisGeom& g, float uc, float vc, float fos, float inv, float dwv,
+                                               int yrow, int mu_min, int mu_max, int mv_min, int mv_max,
+                                               const Read& read, float& acc, float& dacc) {
   const int mu0 = max((int)ceilf((uc - g.hu) * fos - 0.5f), mu_min);
   const int mu1 = min((int)floorf((uc + g.hu) * fos - 0.5f), mu_max);
   const int mv0 = max((int)ceilf((vc - g.hv) * fos - 0.5f), mv_min);
@@ -426,37 +563,26 @@ __device__ __forceinline__ void axis_sums(const AxisGeom& g, float uc, float vc,
   const int cnt = mv1 - mv0 + 1;
   auto row = [&](int mu) {
     const float du = ((float)mu + 0.5f) * inv - uc;
-    const float w = du * g.wu + dv0 * g.wv, dy = du * g.yu + dv0 * g.yv;
+    const float w = du * g.wu + dv0 * g.wv;
     auto body = [&](int j) {
-      const float ww = fmaf((float)j, dwv, w), yy = fmaf((float)j, dyv, dy);
+      const float ww = fmaf((float)j, dwv, w);
+      const float2 s = read(mu, mv0 + j);
       float L = fminf(g.L0, fmaxf(0.f, fmaf(-fabsf(ww), g.K, g.w1K)));
-      L = fabsf(yy) <= g.hby ? L : 0.f;
-      if (!SKIP || L > 0.f) {
-        a = fmaf(read(mu, mv0 + j), L, a);
-        da += L;
-      }
+      L = __float_as_int(s.y) == yrow ? L : 0.f;
+      a = fmaf(s.x, L, a);
+      da += L;
     };
-    if (SKIP) {
-#pragma unroll 1
-      for (int j = 0; j < cnt; ++j) body(j);
-    } else {
 #pragma unroll
-      for (int j = 0; j < 3; ++j)
-        if (j < cnt) body(j);
+    for (int j = 0; j < 3; ++j)
+      if (j < cnt) body(j);
 #pragma unroll 1
-      for (int j = 3; j < cnt; ++j) body(j);
-    }
+    for (int j = 3; j < cnt; ++j) body(j);
   };
-  if (SKIP) {
-#pragma unroll 1
-    for (int r = 0; r < rows; ++r) row(mu0 + r);
-  } else {
 #pragma unroll
-    for (int r = 0; r < 2; ++r)
-      if (r < rows) row(mu0 + r);
+  for (int r = 0; r < 2; ++r)
+    if (r < rows) row(mu0 + r);
 #pragma unroll 1
-    for (int r = 2; r < rows; ++r) row(mu0 + r);
-  }
+  for (int r = 2; r < rows; ++r) row(mu0 + r);
   acc = a;
   dacc = da;
 }
@@ -471,7 +597,8 @@ __device__ __forceinline__ void axis_sums(const AxisGeom& g, float uc, float vc,
 // value is formed from it exactly as sample_interior forms it (x then y),
 // and the samples are weighted by their chords. Returns false (nothing
 // accumulated) when the shadow holds more than 3 samples along an axis.
-__device__ __forceinline__ bool axis_sums_os2(const AxisGeom& g, float uc, float vc, float dwv, float dyv, int mu_min,
+__device__ __forceinline__ bool axis_sums_os2(const AxisGeom& g, float uc, float vc, float dwv,
+                                              const RowAnchor& anchor, int mu_min,
                                               int mu_max, int mv_min, int mv_max, const float* __restrict__ img,
                                               size_t sx, size_t sy, int pw, int ph, float& acc, float& dacc) {
   const int mu0 = max((int)ceilf((uc - g.hu) * 2.0f - 0.5f), mu_min);
@@ -506,17 +633,17 @@ __device__ __forceinline__ bool axis_sums_os2(const AxisGeom& g, float uc, float
     C[2][r] = (1.0f - a2) * T[1][r] + a2 * T[2][r];
   }
   const float du0 = ((float)mu0 + 0.5f) * 0.5f - uc, dv0 = ((float)mv0 + 0.5f) * 0.5f - vc;
-  const float w0 = du0 * g.wu + dv0 * g.wv, y0 = du0 * g.yu + dv0 * g.yv;
-  const float dwu = 0.5f * g.wu, dyu = 0.5f * g.yu;
+  const float w0 = du0 * g.wu + dv0 * g.wv, y0 = anchor.at(g, mu0, mv0);
+  const float dwu = 0.5f * g.wu;
   float a = 0.f, da = 0.f;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       const float ww = fmaf((float)j, dwv, fmaf((float)i, dwu, w0));
-      const float yy = fmaf((float)j, dyv, fmaf((float)i, dyu, y0));
+      const float yy = fmaf((float)j, g.r.v, fmaf((float)i, g.r.u, y0));
       float L = fminf(g.L0, fmaxf(0.f, fmaf(-fabsf(ww), g.K, g.w1K)));
-      L = (fabsf(yy) <= g.hby && i < nu && j < nv) ? L : 0.f;
+      L = (fabsf(yy) < g.hby && i < nu && j < nv) ? L : 0.f;
       const float bj = j == 0 ? b0 : (j == 1 ? b1 : b2);
       const float lo = j == 0 ? C[i][0] : (j == 1 ? (ov ? C[i][0] : C[i][1]) : C[i][1]);
       const float hi = j == 0 ? C[i][1] : (j == 1 ? (ov ? C[i][1] : C[i][2]) : C[i][2]);

@@ -394,16 +394,334 @@ __global__ void __launch_bounds__(32 * NW, 24 / NW) k_slicer_fused(KConst c, con
   }
 }
 
+// ---------------------------------------------------------------------------
+// Single-axis series: k_project_axis, k_slicer_axis.
+//
+// Every ray of a single-axis projection moves in the x-z plane with the same
+// direction, so the major axis of the layer walk and the signs of both steps
+// are the same for all rays of a launch: they become template parameters
+// (ZMAJ, SM, SN), and the host picks the instance from the beam direction.
+// The walk is layer_sum_xz's (same sample bookkeeping, cell sums and order)
+// with cheaper loads: it keeps the near row of the current layer (3 corner
+// values, interpolated in y) and loads the far row at 4 minor positions, so
+// that after a minor crossing the next layer's near row is the far row moved
+// by one. While the 4 positions and the far row lie inside the volume, the
+// far-row corners are read through one running pointer per y plane at fixed
+// offsets (compile-time offsets for the z-major walk), without clamping or
+// index arithmetic; at the volume's faces the walk takes clamped reads.
+
+template <int VT>
+__device__ __forceinline__ float ldv(const char* p) {
+  if (VT == ESB_VOXEL_F32) return __ldg((const float*)p);
+  if (VT == ESB_VOXEL_F16) return __half2float(__ldg((const __half*)p));
+  return __bfloat162float(__ldg((const __nv_bfloat16*)p));
+}
+
+// Sum of the trilinear interpolant over samples j0 .. J-1 of one ray whose y
+// interpolation coordinate lies in cell iy with weight b, walked along major
+// axis z (ZMAJ) or x with step signs SM (major) and SN (minor). Mq, Nq,
+// dM, dN: mirrored major / minor coordinate of sample 0 and |steps|
+// (dM >= dN).
+template <int VT, bool ZMAJ, int SM, int SN>
+__device__ float axis_walk(const Cell<VT>& C, float Mq, float Nq, float dM, float dN, float b, int iy, int j0,
+                           int J) {
+  constexpr long ES = VT == ESB_VOXEL_F32 ? 4 : 2;
+  const long sM = ZMAJ ? C.sz : 1, sN = ZMAJ ? 1 : C.sz;  // element strides of the major and minor axes
+  const int nM = ZMAJ ? C.nz : C.nx, nN = ZMAJ ? C.nx : C.nz;
+  const char* const base = (const char*)C.vol;
+  const float fj0 = (float)j0;
+  const float pM = __fmaf_rn(fj0, dM, Mq), pN = __fmaf_rn(fj0, dN, Nq);
+  float fcm = floorf(pM), fcn = floorf(pN);
+  const float inf = FLT_MAX;
+  const float isM = 1.0f / dM;
+  const float isN = dN > 0.f ? 1.0f / dN : inf;
+  float nMs = ((fcm + 1.f) - pM) * isM;
+  float nNs = dN > 0.f ? ((fcn + 1.f) - pN) * isN : inf;
+  const float g = dN * dM * (1.0f / 12.0f);
+  const float jb = fj0 - 0.5f;
+  const float Mt = (float)(J - j0);
+  const float ib = 1.0f - b;
+  const int ny = C.ny;
+  const long y0 = (long)(iy < 0 ? 0 : (iy > ny - 1 ? ny - 1 : iy)) * C.sy;
+  const long y1 = (long)(iy + 1 < 0 ? 0 : (iy + 1 > ny - 1 ? ny - 1 : iy + 1)) * C.sy;
+  // original indices: far major row of the current layer, first minor position of the window
+  int im = SM * ((int)fcm + 1), in0 = SN * (int)fcn;
+  const char* P = base + ES * (y0 + (long)im * sM + (long)in0 * sN);  // far row, plane iy
+  const long dy = ES * (y1 - y0);
+  const long strideN = SN * ES * sN, strideM = SM * ES * sM;
+  auto ld = [&](int mi, int ni) -> float {  // clamped, interpolated in y
+    mi = mi < 0 ? 0 : (mi > nM - 1 ? nM - 1 : mi);
+    ni = ni < 0 ? 0 : (ni > nN - 1 ? nN - 1 : ni);
+    const char* p = base + ES * ((long)mi * sM + (long)ni * sN + y0);
+    return fmaf(b, ldv<VT>(p + dy), ib * ldv<VT>(p));
+  };
+  // raw far-row values (plane iy, plane iy + 1 at minor positions 0..3)
+  // of the layer whose far row is at major index mi and window start ni
+  const bool canN = nN >= 4;
+  float r0, r1, r2, r3, r4, r5, r6, r7;
+  auto fetch = [&](int mi, int ni, const char* q) {
+    const int lo = SN > 0 ? ni : ni - 3;
+    if (canN && (unsigned)lo <= (unsigned)(nN - 4) && (unsigned)mi < (unsigned)nM) {
+      r0 = ldv<VT>(q);
+      r1 = ldv<VT>(q + dy);
+      r2 = ldv<VT>(q + strideN);
+      r3 = ldv<VT>(q + strideN + dy);
+      r4 = ldv<VT>(q + 2 * strideN);
+      r5 = ldv<VT>(q + 2 * strideN + dy);
+      r6 = ldv<VT>(q + 3 * strideN);
+      r7 = ldv<VT>(q + 3 * strideN + dy);
+    } else {
+      mi = mi < 0 ? 0 : (mi > nM - 1 ? nM - 1 : mi);
+      const char* row = base + ES * ((long)mi * sM + y0);
+      auto at = [&](int n) {
+        n = n < 0 ? 0 : (n > nN - 1 ? nN - 1 : n);
+        return row + ES * ((long)n * sN);
+      };
+      const char* q0 = at(ni);
+      const char* q1 = at(ni + SN);
+      const char* q2 = at(ni + 2 * SN);
+      const char* q3 = at(ni + 3 * SN);
+      r0 = ldv<VT>(q0);
+      r1 = ldv<VT>(q0 + dy);
+      r2 = ldv<VT>(q1);
+      r3 = ldv<VT>(q1 + dy);
+      r4 = ldv<VT>(q2);
+      r5 = ldv<VT>(q2 + dy);
+      r6 = ldv<VT>(q3);
+      r7 = ldv<VT>(q3 + dy);
+    }
+  };
+  // near row of the first layer, and its far row
+  float N0 = ld(im - SM, in0), N1 = ld(im - SM, in0 + SN), N2 = ld(im - SM, in0 + 2 * SN);
+  fetch(im, in0, P);
+  float F0 = fmaf(b, r1, ib * r0), F1 = fmaf(b, r3, ib * r2), F2 = fmaf(b, r5, ib * r4), F3 = fmaf(b, r7, ib * r6);
+  float fm0 = 0.0f, acc = 0.0f;
+#pragma unroll 1
+  for (int guard = 0; guard < 1 << 20; ++guard) {
+    // samples [fm0, fmA) lie in cell (n, m), [fmA, fmL) in cell (n + 1, m)
+    const float fmL = fminf(ceilf(nMs), Mt);
+    const bool X = nNs <= nMs;
+    const float fmA = fmaxf(fminf(ceilf(fminf(nNs, nMs)), Mt), fm0);
+    // the next layer's far row, one minor position further when this layer
+    // crosses: its loads are in flight during this layer's sums
+    const char* Pn = P + strideM + (X ? strideN : 0);
+    const int imn = im + SM, in0n = in0 + (X ? SN : 0);
+    fetch(imn, in0n, Pn);
+    {  // cell (n, m): near corners N0, N1, far corners F0, F1
+      const float M = fmA - fm0;
+      const float jm = __fmaf_rn(0.5f, fm0 + fmA, jb);
+      const float a = __fmaf_rn(jm, dN, Nq) - fcn, c = __fmaf_rn(jm, dM, Mq) - fcm;
+      const float k1 = N1 - N0, k3 = F0 - N0, k5 = (F1 - F0) - k1;
+      const float f = fmaf(c, fmaf(a, k5, k3), fmaf(a, k1, N0));
+      acc = fmaf(M, fmaf(k5, fmaf(M * M, g, -g), f), acc);
+    }
+    {  // cell (n + 1, m): near corners N1, N2, far corners F1, F2
+      const float M = fmL - fmA;
+      const float jm = __fmaf_rn(0.5f, fmA + fmL, jb);
+      const float a = __fmaf_rn(jm, dN, Nq) - (fcn + 1.f), c = __fmaf_rn(jm, dM, Mq) - fcm;
+      const float k1 = N2 - N1, k3 = F1 - N1, k5 = (F2 - F1) - k1;
+      const float f = fmaf(c, fmaf(a, k5, k3), fmaf(a, k1, N1));
+      acc = fmaf(M, fmaf(k5, fmaf(M * M, g, -g), f), acc);
+    }
+    fm0 = fmL;
+    if (fm0 >= Mt) break;
+    // next layer
+    N0 = X ? F1 : F0;
+    N1 = X ? F2 : F1;
+    N2 = X ? F3 : F2;
+    F0 = fmaf(b, r1, ib * r0);
+    F1 = fmaf(b, r3, ib * r2);
+    F2 = fmaf(b, r5, ib * r4);
+    F3 = fmaf(b, r7, ib * r6);
+    if (X) {
+      fcn += 1.f;
+      nNs = ((fcn + 1.f) - pN) * isN;
+    }
+    fcm += 1.f;
+    nMs = ((fcm + 1.f) - pM) * isM;
+    im = imn;
+    in0 = in0n;
+    P = Pn;
+  }
+  return acc;
+}
+
+// Sum over the samples of one sub-ray from t0 to tout (ray_sum) with the
+// axis walk when the ray fits the launch's instance (its y in one cell, its
+// major axis and step signs the instance's), else ray_sum's walkers.
+template <int VT, bool ZMAJ, int SM, int SN>
+__device__ float axis_ray_sum(const KConst& c, const Cell<VT>& C, float3 s, float t0, float tout,
+                              bool first_at_source) {
+  if (!(t0 <= tout)) return 0.0f;
+  const float h = c.vs.x * 0.15f;
+  float step;
+  bool ok;
+  const int J = progression(t0, tout, h, step, ok);
+  if (!ok) return ray_sum<VT, unsigned long long>(c, C, s, t0, tout, first_at_source);
+  const float3 q0 = interp_coord(c, ray_point(c, s, t0));
+  const float3 dq = interp_step(c, step);
+  float sum = 0.0f;
+  int j0 = 0;
+  if (first_at_source) {
+    const float3 q = interp_coord(c, s);
+    sum = trilinear<VT>(C, q.x, q.y, q.z);
+    j0 = 1;
+  }
+  const float ylast = qpos(q0.y, J - 1, dq.y);
+  if (!(fabsf(dq.y) * (float)J < 1e-5f && floorf(q0.y) == floorf(ylast)))
+    return sum + cell_sum<VT>(C, q0.x, q0.y, q0.z, dq.x, dq.y, dq.z, j0, J);
+  const float fy = floorf(q0.y);
+  const float qm = ZMAJ ? q0.z : q0.x, dqm = ZMAJ ? dq.z : dq.x;
+  const float qn = ZMAJ ? q0.x : q0.z, dqn = ZMAJ ? dq.x : dq.z;
+  if ((fabsf(dq.z) >= fabsf(dq.x)) != ZMAJ || (dqm < 0.f ? -1 : 1) != SM || (dqn < 0.f ? -1 : 1) != SN)
+    return sum + cell_sum_xz<VT, unsigned long long>(C, q0.x, q0.y - fy, (int)fy, q0.z, dq.x, dq.z, j0, J);
+  if (j0 >= J) return sum;
+  return sum + axis_walk<VT, ZMAJ, SM, SN>(C, SM > 0 ? qm : -qm, SN > 0 ? qn : -qn, fabsf(dqm), fabsf(dqn),
+                                           q0.y - fy, (int)fy, j0, J);
+}
+
+// k_project_fast (march) for single-axis series; layout of k_project_fast.
+template <int VT, bool ZMAJ, int SM, int SN>
+__global__ void __launch_bounds__(256) k_project_axis(KConst c, const void* __restrict__ vol, float* __restrict__ proj,
+                                                      float* __restrict__ dist, size_t pitchE, int x0, int y0, int x1,
+                                                      int y1) {
+  const int lane = threadIdx.x & 31;
+  const int sub = lane & 3;
+  const int row = lane >> 2;
+  const int nw = blockDim.x >> 5;
+  const int x = x0 + (int)blockIdx.x * nw + (int)(threadIdx.x >> 5);
+  const int y = y0 + (int)blockIdx.y * 8 + row;
+  const bool active = x < x1 && y < y1;
+  Cell<VT> C{vol, (int)c.dim.x, (int)c.dim.y, (int)c.dim.z, (long)c.dim.x, (long)c.dim.x * (long)c.dim.y};
+  float sum = 0.0f, gx = 0.0f, gz = 0.0f;
+  if (active) {
+    const float osx = (sub & 2) ? 0.75f : 0.25f, osy = (sub & 1) ? 0.75f : 0.25f;
+    const float3 s = ray_src(c, (float)x + osx, (float)y + osy);
+    float tin, tout;
+    hit(s, c.n, c.bbMin, c.bbMax, tin, tout);
+    if (tout - tin > 0.0f) {
+      gx = 1.0f;
+      gz = tout - tin;
+      sum = axis_ray_sum<VT, ZMAJ, SM, SN>(c, C, s, tin, tout, false);
+    }
+  }
+  sum = quad_sum_ordered(sum);
+  gx = quad_sum_ordered(gx);
+  gz = quad_sum_ordered(gz);
+  if (active && sub == 0) {
+    const size_t i = (size_t)y * pitchE + x;
+    proj[i] += sum * c.vs.x * 0.15f * 0.25f;
+    dist[i] = fmaxf(0.0f, gz / gx);
+  }
+}
+
+// k_slicer_fused for single-axis series; layout of k_slicer_fused.
+template <int VT, bool ZMAJ, int SM, int SN>
+__global__ void __launch_bounds__(256) k_slicer_axis(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
+                                                     size_t img_stride, size_t pitchE, SlabTable slabs, int x0, int y0,
+                                                     int x1, int y1) {
+  const int lane = threadIdx.x & 31;
+  const int sub = lane & 3;
+  const int row = lane >> 2;
+  const int nw = blockDim.x >> 5;
+  const int x = x0 + (int)blockIdx.x * nw + (int)(threadIdx.x >> 5);
+  const int y = y0 + (int)blockIdx.y * 8 + row;
+  const bool active = x < x1 && y < y1;
+  Cell<VT> C{vol, (int)c.dim.x, (int)c.dim.y, (int)c.dim.z, (long)c.dim.x, (long)c.dim.x * (long)c.dim.y};
+  float3 s = make_float3(0.f, 0.f, 0.f);
+  float tin = 0.f, tout = -1.f;
+  int klo = ESB_MAX_SLABS, khi = -1;
+  bool hitray = false;
+  if (active) {
+    const float osx = (sub & 2) ? 0.75f : 0.25f, osy = (sub & 1) ? 0.75f : 0.25f;
+    s = ray_src(c, (float)x + osx, (float)y + osy);
+    hit(s, c.n, c.bbMin, c.bbMax, tin, tout);
+    hitray = tout - tin > 0.0f;
+    if (hitray) {
+      for (int k = 0; k < slabs.count; ++k) {
+        // slab k has samples when max(tin, b_k) <= min(tout, b_{k+1})
+        if (fmaxf(tin, slabs.bound[k]) <= fminf(tout, slabs.bound[k + 1])) {
+          klo = min(klo, k);
+          khi = max(khi, k);
+        }
+      }
+    }
+  }
+  for (int o = 1; o <= 2; o <<= 1) {
+    klo = min(klo, __shfl_xor_sync(0xffffffffu, klo, o));
+    khi = max(khi, __shfl_xor_sync(0xffffffffu, khi, o));
+  }
+  // the warp walks the union of its pixels' slab ranges (shuffles need all lanes)
+  int wlo = klo, whi = khi;
+  for (int o = 4; o <= 16; o <<= 1) {
+    wlo = min(wlo, __shfl_xor_sync(0xffffffffu, wlo, o));
+    whi = max(whi, __shfl_xor_sync(0xffffffffu, whi, o));
+  }
+  const size_t pix = (size_t)y * pitchE + x;
+  for (int k = wlo; k <= whi; ++k) {
+    float v = 0.0f;
+    if (hitray && k >= klo && k <= khi)
+      v = axis_ray_sum<VT, ZMAJ, SM, SN>(c, C, s, fmaxf(tin, slabs.bound[k]), fminf(tout, slabs.bound[k + 1]), true);
+    v = quad_sum_ordered(v);
+    if (active && sub == 0 && k >= klo && k <= khi) imgs[(size_t)k * img_stride + pix] = v * c.vs.x * 0.15f * 0.25f;
+  }
+}
+
+// Beam directions whose rays all stay in one y plane take the axis kernels.
+bool axis_projection(const KConst& c) { return fabsf(c.n.y) <= 1e-6f; }
+
+// Instance of the axis kernels for the launch's beam direction: major axis z
+// when |dq.z| >= |dq.x| (as each ray decides it), step signs.
+void axis_orientation(const KConst& c, bool& zmaj, int& sm, int& sn) {
+  const float qx = c.n.x * c.bbRcp.x * c.dim.x, qz = c.n.z * c.bbRcp.z * c.dim.z;
+  zmaj = fabsf(qz) >= fabsf(qx);
+  const float m = zmaj ? qz : qx, n = zmaj ? qx : qz;
+  sm = m < 0.f ? -1 : 1;
+  sn = n < 0.f ? -1 : 1;
+}
+
 // Volumes of 2^32 voxels or more take 64-bit element offsets in the walk.
 bool big_volume(const KConst& c) { return (double)c.dim.x * c.dim.y * c.dim.z > 4294967295.0; }
 
 }  // namespace
 
 // nw: warps per block (2, 4 or 8; 64-bit-offset volumes always take 4).
+
+// One launch of an axis kernel instance per beam orientation.
+#define ESB_AXIS_ORIENT(KER, VT, GRD, BLK, ST, ...)                              \
+  do {                                                                          \
+    bool zmaj_;                                                                 \
+    int sm_, sn_;                                                               \
+    axis_orientation(c, zmaj_, sm_, sn_);                                       \
+    const int o_ = (zmaj_ ? 4 : 0) + (sm_ > 0 ? 2 : 0) + (sn_ > 0 ? 1 : 0);     \
+    switch (o_) {                                                               \
+      case 0: KER<VT, false, -1, -1><<<GRD, BLK, 0, ST>>>(__VA_ARGS__); break;  \
+      case 1: KER<VT, false, -1, 1><<<GRD, BLK, 0, ST>>>(__VA_ARGS__); break;   \
+      case 2: KER<VT, false, 1, -1><<<GRD, BLK, 0, ST>>>(__VA_ARGS__); break;   \
+      case 3: KER<VT, false, 1, 1><<<GRD, BLK, 0, ST>>>(__VA_ARGS__); break;    \
+      case 4: KER<VT, true, -1, -1><<<GRD, BLK, 0, ST>>>(__VA_ARGS__); break;   \
+      case 5: KER<VT, true, -1, 1><<<GRD, BLK, 0, ST>>>(__VA_ARGS__); break;    \
+      case 6: KER<VT, true, 1, -1><<<GRD, BLK, 0, ST>>>(__VA_ARGS__); break;    \
+      default: KER<VT, true, 1, 1><<<GRD, BLK, 0, ST>>>(__VA_ARGS__); break;    \
+    }                                                                           \
+  } while (0)
+
 cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float* imgs, size_t img_stride,
                                 size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1,
                                 cudaStream_t st, int nw) {
   if (x1 <= x0 || y1 <= y0 || slabs.count <= 0) return cudaSuccess;
+  if (axis_projection(c)) {  // the axis walk, one sub-ray per thread
+    if (nw != 2 && nw != 8) nw = 4;
+    dim3 blk(32 * nw), grd((x1 - x0 + nw - 1) / nw, (y1 - y0 + 7) / 8);
+    if (vt == ESB_VOXEL_F32)
+      ESB_AXIS_ORIENT(k_slicer_axis, ESB_VOXEL_F32, grd, blk, st, c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
+    else if (vt == ESB_VOXEL_F16)
+      ESB_AXIS_ORIENT(k_slicer_axis, ESB_VOXEL_F16, grd, blk, st, c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
+    else
+      ESB_AXIS_ORIENT(k_slicer_axis, ESB_VOXEL_BF16, grd, blk, st, c, vol, imgs, img_stride, pitchE, slabs, x0, y0, x1, y1);
+    ESB_COUNT_LAUNCH();
+    return cudaGetLastError();
+  }
   const bool big = big_volume(c);
   if (big || (nw != 2 && nw != 8)) nw = 4;
   dim3 blk(32 * nw), grd((x1 - x0 + nw - 1) / nw, (y1 - y0 + 7) / 8);
@@ -429,6 +747,18 @@ cudaError_t launch_project_fast(const KConst& c, const void* vol, int vt, int mo
                                 size_t pitchE, float tmin, float tmax, int x0, int y0, int x1, int y1,
                                 cudaStream_t st, int nw) {
   if (x1 <= x0 || y1 <= y0) return cudaSuccess;
+  if (mode == 0 && axis_projection(c)) {  // the axis walk, one sub-ray per thread
+    if (nw != 2 && nw != 8) nw = 4;
+    dim3 blk(32 * nw), grd((x1 - x0 + nw - 1) / nw, (y1 - y0 + 7) / 8);
+    if (vt == ESB_VOXEL_F32)
+      ESB_AXIS_ORIENT(k_project_axis, ESB_VOXEL_F32, grd, blk, st, c, vol, proj, dist, pitchE, x0, y0, x1, y1);
+    else if (vt == ESB_VOXEL_F16)
+      ESB_AXIS_ORIENT(k_project_axis, ESB_VOXEL_F16, grd, blk, st, c, vol, proj, dist, pitchE, x0, y0, x1, y1);
+    else
+      ESB_AXIS_ORIENT(k_project_axis, ESB_VOXEL_BF16, grd, blk, st, c, vol, proj, dist, pitchE, x0, y0, x1, y1);
+    ESB_COUNT_LAUNCH();
+    return cudaGetLastError();
+  }
   const bool big = big_volume(c);
   if (big || (nw != 2 && nw != 8)) nw = 4;
   dim3 blk(32 * nw), grd((x1 - x0 + nw - 1) / nw, (y1 - y0 + 7) / 8);

@@ -104,13 +104,15 @@ __global__ void __launch_bounds__(kQuadsPerItem, 5) k_subvol_batch(const SubvolW
                           : sample_image(img, pw, ph, (size_t)pw, px, py, lin, true);
         };
         const bool patch = os == 2 && lin && interior;
+        const float cx0 = pc.k.bbMin.x + ((float)x + 0.5f) * pc.k.vs.x;
+        const RowAnchor anchor(ag, y, ag.U.x * cx0 + uyz, ag.V.x * cx0 + vyz, (float)os);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const float cx = pc.k.bbMin.x + ((float)(x + i) + 0.5f) * pc.k.vs.x;
           const float uc = ag.U.x * cx + uyz, vc = ag.V.x * cx + vyz;
-          if (!(patch && axis_sums_os2(ag, uc, vc, inv * ag.wv, inv * ag.yv, pbx * 2, pby * 2 - 1, pbz * 2,
+          if (!(patch && axis_sums_os2(ag, uc, vc, inv * ag.wv, anchor, pbx * 2, pby * 2 - 1, pbz * 2,
                                        pbw * 2 - 1, img, (size_t)ph, 1, pw, ph, acc[i], dacc[i])))
-            axis_sums<true>(ag, uc, vc, (float)os, inv, inv * ag.wv, inv * ag.yv, pbx * os, pby * os - 1, pbz * os,
+            axis_sums(ag, uc, vc, (float)os, inv, inv * ag.wv, anchor, pbx * os, pby * os - 1, pbz * os,
                             pbw * os - 1, read, acc[i], dacc[i]);
         }
       } else {
