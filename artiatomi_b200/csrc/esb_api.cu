@@ -104,6 +104,7 @@ static thread_local std::string g_last_error;
 static std::atomic<unsigned long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+static void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 int fail(int code, const std::string& msg) {
@@ -456,6 +457,17 @@ struct esb_reconstructor {
   bool r2c_many_ok[ESB_CTF_SLAB_BATCH + 1] = {};
   bool graphs = false;                   // replay SART iterations from a captured graph
   cudaGraphExec_t sart_exec = nullptr;   // the last captured iteration
+  // inputs the captured iteration was recorded with (it replays only for the
+  // same ones) and the library kernels it launches
+  struct {
+    const void* vol = nullptr;
+    int voxel_type = -1;
+    const float* projections = nullptr;
+    esb_vol_geom vg{};
+    std::vector<int> index_list;
+    int sirt_count = 0;
+  } sart_key;
+  unsigned long long sart_graph_launches = 0;
   cudaStream_t capture_stream = nullptr;  // private stream the capture records on
   // projection preparation: square, spectrum and plans when CTF is off,
   // the converted / windowed image and the statistics
@@ -1529,45 +1541,69 @@ int esb_sart_run(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int vo
   }
   int rc;
   int iter = 0;
-  if (r->graphs && !r->timing && iterations > 1) {
-    // The first iteration runs eagerly: it sizes every buffer (slab images,
-    // FFT plans) and settles volume_is_empty. One more iteration is captured
-    // on the stream and the rest replay it.
-    if ((rc = sart_iteration(r, vg, vol, voxel_type, projections, index_list, proj_count, sirt_count,
-                             volume_is_empty)))
-      return rc;
-    ++iter;
-    if (r->sart_exec) {
-      ESB_CK(cudaStreamSynchronize(r->stream), "esb_sart_run");
-      cudaGraphExecDestroy(r->sart_exec);
-      r->sart_exec = nullptr;
+  if (r->graphs && !r->timing && iterations > 0) {
+    // One SART iteration is captured as a CUDA graph and replayed, within
+    // this call and by later calls with the same inputs (the graph holds
+    // their pointers and geometry). A call with other inputs, or one that
+    // starts on an empty volume, first runs an iteration eagerly: it sizes
+    // every buffer (slab images, FFT plans) and settles volume_is_empty;
+    // the next iteration is then captured (recorded, not run).
+    auto& k = r->sart_key;
+    const bool same = r->sart_exec && !*volume_is_empty && k.vol == vol && k.voxel_type == voxel_type &&
+                      k.projections == projections && k.sirt_count == sirt_count &&
+                      memcmp(&k.vg, vg, sizeof(esb_vol_geom)) == 0 && (int)k.index_list.size() == proj_count &&
+                      std::equal(k.index_list.begin(), k.index_list.end(), index_list);
+    if (!same) {
+      if ((rc = sart_iteration(r, vg, vol, voxel_type, projections, index_list, proj_count, sirt_count,
+                               volume_is_empty)))
+        return rc;
+      ++iter;
+      if (r->sart_exec) {
+        ESB_CK(cudaStreamSynchronize(r->stream), "esb_sart_run");
+        cudaGraphExecDestroy(r->sart_exec);
+        r->sart_exec = nullptr;
+      }
+      // The capture records on a private stream (the caller's may be the
+      // legacy default stream, which cannot be captured); the graph is then
+      // launched on the caller's stream.
+      if (!r->capture_stream)
+        ESB_CK(cudaStreamCreateWithFlags(&r->capture_stream, cudaStreamNonBlocking), "esb_sart_run capture");
+      cudaStream_t user = r->stream;
+      if ((rc = esb_reconstructor_set_stream(r, r->capture_stream))) return rc;
+      cudaError_t e = cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) {
+        esb_reconstructor_set_stream(r, user);
+        return cuda_fail(e, "esb_sart_run capture");
+      }
+      const unsigned long long l0 = g_launches.load();
+      rc = sart_iteration(r, vg, vol, voxel_type, projections, index_list, proj_count, sirt_count, volume_is_empty);
+      const unsigned long long captured = g_launches.load() - l0;
+      cudaGraph_t graph = nullptr;
+      e = cudaStreamEndCapture(r->stream, &graph);
+      const int rs = esb_reconstructor_set_stream(r, user);
+      if (!rc) rc = rs;
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      ESB_CK(e, "esb_sart_run capture");
+      const cudaError_t ei = cudaGraphInstantiate(&r->sart_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      ESB_CK(ei, "esb_sart_run instantiate");
+      // the captured launches run when the graph does: counted at each replay
+      g_launches.fetch_sub(captured);
+      r->sart_graph_launches = captured;
+      k.vol = vol;
+      k.voxel_type = voxel_type;
+      k.projections = projections;
+      k.vg = *vg;
+      k.index_list.assign(index_list, index_list + proj_count);
+      k.sirt_count = sirt_count;
     }
-    // The capture records on a private stream (the caller's may be the
-    // legacy default stream, which cannot be captured); the graph is then
-    // launched on the caller's stream.
-    if (!r->capture_stream)
-      ESB_CK(cudaStreamCreateWithFlags(&r->capture_stream, cudaStreamNonBlocking), "esb_sart_run capture");
-    cudaStream_t user = r->stream;
-    if ((rc = esb_reconstructor_set_stream(r, r->capture_stream))) return rc;
-    cudaError_t e = cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) {
-      esb_reconstructor_set_stream(r, user);
-      return cuda_fail(e, "esb_sart_run capture");
+    for (; iter < iterations; ++iter) {
+      ESB_CK(cudaGraphLaunch(r->sart_exec, r->stream), "esb_sart_run replay");
+      count_launches(r->sart_graph_launches);
     }
-    rc = sart_iteration(r, vg, vol, voxel_type, projections, index_list, proj_count, sirt_count, volume_is_empty);
-    cudaGraph_t graph = nullptr;
-    e = cudaStreamEndCapture(r->stream, &graph);
-    const int rs = esb_reconstructor_set_stream(r, user);
-    if (!rc) rc = rs;
-    if (rc) {
-      if (graph) cudaGraphDestroy(graph);
-      return rc;
-    }
-    ESB_CK(e, "esb_sart_run capture");
-    const cudaError_t ei = cudaGraphInstantiate(&r->sart_exec, graph, 0);
-    cudaGraphDestroy(graph);
-    ESB_CK(ei, "esb_sart_run instantiate");
-    for (; iter < iterations; ++iter) ESB_CK(cudaGraphLaunch(r->sart_exec, r->stream), "esb_sart_run replay");
     return ok();
   }
   for (; iter < iterations; ++iter) {

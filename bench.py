@@ -18,6 +18,14 @@ reconstructor's stream between barriers, maximum over ranks.
 --impl reference times the CPU oracle (the multithreaded C++ restatement of
 the reference's kernels; the reference's own GPU code cannot be compiled with
 CUDA 12.9) on a bounded sample of the same workload and prints the same line.
+That arm never loads this library: it reads the workload parameters and the
+phantom generator by path.
+
+The GPU arm replays the SART subset loop from a captured CUDA graph
+(esb_reconstructor_enable_graphs). After the timed steps it reports the
+parity of the same kernels at the C2 geometry cropped to 256x256x64 (rel-L2
+of the reconstructed volume against the FP32 and FP64 CPU oracles), with the
+CPU baseline.
 """
 from __future__ import annotations
 
@@ -34,6 +42,28 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+
+
+def _load_by_path(name: str, rel: str):
+    """A module of the package loaded from its file, without the package's
+    __init__ (which loads the CUDA library)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location(name, ROOT / rel)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config(name: str, params: dict, ws: int = 1) -> dict:
+    """The `config` object of both arms' JSON lines."""
+    vox = params["dims"][0] * params["dims"][1] * params["dims"][2]
+    return {"workload": name, "volume": list(params["dims"]), "projections": params["n_proj"],
+            "projection_size": [params["W"], params["H"]], "oversampling": params["os"],
+            "sirt_count": params["sirt"], "ctf": params["ctf"], "ctf_slab_nm": 30.0 if params["ctf"] else None,
+            "voxel_storage": "f32", "l2": f"inputs larger than L2 (volume {vox * 4 / 2**20:.0f} MiB)",
+            "parallelism": f"replicas x{ws}"}
+
 
 METRIC = "SART voxel-updates/s (SART+3D-CTF iteration, 1024x1024x256, 61x1024^2)"
 UNIT = "voxel-updates/s"
@@ -128,8 +158,8 @@ def cpu_sample(workload_params, n_proj_sample: int = 4, y_extent: int = 8):
     """
     from oracle import geometry as G
     from oracle.driver import OracleReconstructor
-    from oracle import driver as D
-    from artiatomi_b200 import phantom as PH
+
+    PH = _load_by_path("esb_phantom", "artiatomi_b200/phantom.py")
 
     p = workload_params
     nx, ny, nz = p["dims"]
@@ -182,37 +212,56 @@ def cpu_sample(workload_params, n_proj_sample: int = 4, y_extent: int = 8):
     vu = nx * ny * nz / per_proj
     from oracle.lib import NTHREADS
 
-    return vu, dict(per_projection_s=per_proj, sample=f"{len(idx)} projections of the workload on a "
-                    f"{nx}x{y_extent}x{nz} tilt-axis slice (volume {nx}x{ny}x{nz}); voxel work x{scale:.0f}, "
-                    f"CTF chain (1024^2 FFTs) counted once", cores=NTHREADS)
+    return vu, dict(per_projection_s=per_proj, sample_s=t_fp + t_bp,
+                    sample=f"{len(idx)} projections of the workload on a {nx}x{y_extent}x{nz} tilt-axis slice "
+                    f"(volume {nx}x{ny}x{nz}), timed; value extrapolated to the full volume: voxel work x{scale:.0f}, "
+                    f"CTF chains ({max(W, H)}^2 FFTs) counted once", cores=NTHREADS)
 
 
 def run_reference(args):
     ws, rank, _ = _dist_setup()
     if rank != 0:
         return 0
-    from artiatomi_b200.workloads import CONFIGS
-
-    params = CONFIGS[args.workload]
+    params = _load_by_path("esb_configs", "artiatomi_b200/configs.py").CONFIGS[args.workload]
     for _ in range(args.warmup):
         cpu_sample(params, n_proj_sample=1)
-    vals = []
-    t_all = time.perf_counter()
+    vals, secs = [], []
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         v, det = cpu_sample(params, n_proj_sample=2)
+        secs.append(time.perf_counter() - t0)
         vals.append(v)
     value = float(np.median(vals))
-    ms = params["dims"][0] * params["dims"][1] * params["dims"][2] * params["n_proj"] / value * 1e3
+    full_ms = params["dims"][0] * params["dims"][1] * params["dims"][2] * params["n_proj"] / value * 1e3
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "volume": list(params["dims"]), "projections": params["n_proj"],
-                       "oversampling": params["os"], "sirt_count": params["sirt"], "ctf": params["ctf"]},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(secs)) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args.workload, params, ws),
+            "extrapolated": True,
+            "extrapolation": "a step is the bounded sample below (ms_per_step: its measured time); value is the "
+                             "sample's throughput extrapolated to the full workload (full_step_ms_extrapolated)",
+            "full_step_ms_extrapolated": full_ms,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": det["cores"], "kind": "port",
-                             "sample": det["sample"]},
+                             "sample": det["sample"], "sample_s": float(np.mean(secs))},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def config_parity(name: str = "c2_crop") -> dict:
+    """The SART volume of workload `name` (FAST kernels, this library)
+    against the FP32 and FP64 CPU oracles, on the same measured projections."""
+    from oracle.parity import rel_l2, run_config
+
+    t0 = time.perf_counter()
+    run = run_config(name, variants=("fast",), precisions=(0, 1))
+    p = run.params
+    return {"workload": name, "volume": list(p["dims"]), "projections": p["n_proj"], "iterations": p["iterations"],
+            "oversampling": p["os"], "sirt_count": p["sirt"], "ctf": p["ctf"],
+            "rel_l2_vs_fp32_oracle": rel_l2(run.volumes["fast"], run.oracle[0]),
+            "rel_l2_vs_fp64_oracle": rel_l2(run.volumes["fast"], run.oracle[1]),
+            "fp32_oracle_vs_fp64_oracle": rel_l2(run.oracle[0], run.oracle[1]),
+            "seconds": round(time.perf_counter() - t0, 1)}
 
 
 def run_esb(args):
@@ -236,6 +285,8 @@ def run_esb(args):
 
     cfg = dataclasses.replace(wl.cfg, variant=E.VARIANT_FAST if args.variant == "fast" else E.VARIANT_FAITHFUL)
     rec = E.Reconstructor(cfg, wl.pg, wl.tilt, wl.defocus, stream=stream)
+    graphs = not args.no_graphs
+    rec.enable_graphs(graphs)  # the subset loop replays from a captured CUDA graph
     vol = torch.zeros(params["dims"][::-1], dtype=torch.float32, device=dev)
     sirt = params["sirt"]
 
@@ -269,9 +320,9 @@ def run_esb(args):
     gpu_launches = E.kernel_launches() - launches0
     barrier()
 
-    # ---- per-phase device time and launch-group counts: one more step with
-    # an event pair around every launch group (kept out of the timed steps,
-    # where the events would add host work per launch)
+    # ---- per-phase device time and launch-group counts: one more step, run
+    # eagerly with an event pair around every launch group (kept out of the
+    # timed steps, where the events would add host work per launch)
     rec.enable_timing(True)
     rec.timing()
     with torch.cuda.stream(stream):
@@ -329,22 +380,22 @@ def run_esb(args):
     achieved = bytes_unit / (t_unit * 1e-3) / 1e9
 
     cpu = None
+    parity = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, det = cpu_sample(params, n_proj_sample=1)
-        cpu = {"value": v, "unit": UNIT, "cores": det["cores"], "kind": "port", "sample": det["sample"]}
+        cpu = {"value": v, "unit": UNIT, "cores": det["cores"], "kind": "port", "sample": det["sample"],
+               "extrapolated": True}
+        if args.workload.startswith("c2_"):
+            parity = config_parity("c2_crop")
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid+bead phantom, "
                 "projections from this library's projector + noise)",
-                "config": {"workload": args.workload, "volume": list(params["dims"]),
-                           "projections": params["n_proj"], "projection_size": [params["W"], params["H"]],
-                           "oversampling": params["os"], "sirt_count": sirt, "ctf": params["ctf"],
-                           "ctf_slab_nm": 30.0, "voxel_storage": "f32", "kernels": args.variant,
-                           "l2": f"inputs larger than L2 (volume {wl.voxels * 4 / 2**20:.0f} MiB)",
-                           "parallelism": f"replicas x{ws}",
-                           "launch_shapes": E.autotune_report().strip().splitlines()},
+                "config": workload_config(args.workload, params, ws),
+                "kernels": args.variant, "graphs": graphs,
+                "launch_shapes": E.autotune_report().strip().splitlines(),
                 "e2e": {"value": e2e_value, "unit": UNIT,
                         "h2d_bytes_per_step": int(wl.projections.numel() * 4),
                         "d2h_bytes_per_step": int(vol.numel() * 4)},
@@ -357,7 +408,8 @@ def run_esb(args):
                              "launches": launches},
                 "phases_ms_per_step": {k: v[0] for k, v in phases.items()},
                 "clocks": clk.summary(),
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu,
+                "parity": parity}
         print(json.dumps(line), flush=True)
     rec.close()
     if ws > 1:
@@ -373,7 +425,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["esb", "reference"], default="esb")
     ap.add_argument("--workload", default="c2_sart_ctf")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline and the oracle parity of the C2 crop")
+    ap.add_argument("--no-graphs", action="store_true", help="launch the subset loop eagerly")
     ap.add_argument("--variant", choices=["fast", "faithful"], default="fast",
                     help="fast: closed-form cell-sum projector and per-voxel-shadow back-projector; "
                          "faithful: the reference's per-sample arithmetic")
