@@ -36,6 +36,7 @@ UNITS = [
     ("esb_refine.cu", []),
     ("esb_cc.cu", ["--fmad=false"]),
     ("esb_image.cu", ["--fmad=false"]),
+    ("esb_ctf.cu", []),
     ("esb_api.cu", []),
     ("esb_noalloc.cu", []),
     ("esb_geometry.cpp", []),
