@@ -123,11 +123,15 @@ _SIGS = {
     "esb_rec_compare": ([P, C.POINTER(VolGeom), P, I], I),
     "esb_rec_back_projection": ([P, C.POINTER(VolGeom), P, I, I, F], I),
     "esb_sart_run": ([P, C.POINTER(VolGeom), P, I, P, P, I, I, I, C.POINTER(I)], I),
+    "esb_sart_run_zslab": ([P, C.POINTER(VolGeom), P, I, P, P, I, I, I, C.POINTER(I), P, P], I),
     "esb_subvolume_wbp": ([P, C.POINTER(VolGeom), I, P, P, P, P, P, P, I, I], I),
     "esb_sart_projection_update_noalloc": ([C.POINTER(ReconConfig), C.POINTER(ProjGeom), C.POINTER(VolGeom), P, P, P,
                                             I, P, F, I, P], I),
 }
 NOALLOC_MAX_PIXELS = 2048 * 2048
+
+# esb_allreduce_fn: int (*)(float* buf, size_t count, void* stream, void* user)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p)
 
 
 def header_symbols() -> list[str]:

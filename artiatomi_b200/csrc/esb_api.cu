@@ -498,8 +498,10 @@ struct PhaseScope {
 
 static int rec_alloc(esb_reconstructor* r) {
   const size_t img = (size_t)r->cfg.proj_x * r->cfg.proj_y * sizeof(float);
-  ESB_CK(cudaMalloc(&r->proj_d, img), "esb_reconstructor_create");
-  ESB_CK(cudaMalloc(&r->dist_d, img), "esb_reconstructor_create");
+  // the projection and the ray-length image are one buffer (projection
+  // first), so that a z-slab run sums both over ranks in one collective
+  ESB_CK(cudaMalloc(&r->proj_d, 2 * img), "esb_reconstructor_create");
+  r->dist_d = r->proj_d + (size_t)r->cfg.proj_x * r->cfg.proj_y;
   ESB_CK(cudaMalloc(&r->real_d, img), "esb_reconstructor_create");
   ESB_CK(cudaMemset(r->proj_d, 0, img), "esb_reconstructor_create");
   ESB_CK(cudaMemset(r->dist_d, 0, img), "esb_reconstructor_create");
@@ -515,8 +517,7 @@ static int rec_alloc(esb_reconstructor* r) {
 }
 
 static void rec_free(esb_reconstructor* r) {
-  cudaFree(r->proj_d);
-  cudaFree(r->dist_d);
+  cudaFree(r->proj_d);  // with dist_d
   cudaFree(r->real_d);
   cudaFree(r->square_d);
   cudaFree(r->fft_d);
@@ -1610,6 +1611,53 @@ int esb_sart_run(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int vo
     if ((rc = sart_iteration(r, vg, vol, voxel_type, projections, index_list, proj_count, sirt_count,
                              volume_is_empty)))
       return rc;
+  }
+  return ok();
+}
+
+int esb_sart_run_zslab(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type,
+                       const float* projections, const int* index_list, int proj_count, int iterations, int sirt_count,
+                       int* volume_is_empty, esb_allreduce_fn allreduce, void* user) {
+  const char* where = "esb_sart_run_zslab";
+  if (!r || !vg || !vol || !projections || !index_list || !volume_is_empty || !valid_vt(voxel_type) || !allreduce)
+    return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": NULL argument");
+  if (proj_count <= 0 || iterations < 0 || sirt_count < 1)
+    return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": invalid counts");
+  for (int i = 0; i < proj_count; ++i)
+    if (index_list[i] < 0 || index_list[i] >= r->cfg.n_proj)
+      return fail(ESB_ERR_INVALID_ARGUMENT, std::string(where) + ": index list entry out of range");
+  const size_t img = (size_t)r->cfg.proj_x * r->cfg.proj_y;
+  while ((int)r->sirt_d.size() < sirt_count) {
+    float* p = nullptr;
+    ESB_CK(cudaMalloc(&p, img * sizeof(float)), where);
+    r->sirt_d.push_back(p);
+  }
+  int rc;
+  const int steps = (proj_count + sirt_count - 1) / sirt_count;
+  for (int it = 0; it < iterations; ++it) {
+    for (int s = 0; s < steps; ++s) {
+      for (int i = 0; i < sirt_count; ++i) {
+        if (s * sirt_count + i >= proj_count) continue;
+        const int index = index_list[s * sirt_count + i];
+        if ((rc = esb_rec_reset_projections(r))) return rc;
+        if ((rc = esb_rec_forward_projection(r, vg, vol, voxel_type, index, *volume_is_empty))) return rc;
+        // the slab's line integrals and ray lengths, summed over the ranks in
+        // one collective on the stream (Reconstructor.cpp:440-463 gathers
+        // both on rank 0 and EmSart.cpp:647 broadcasts the residuals; with
+        // the sums on every rank each forms the same residual itself)
+        if ((rc = allreduce(r->proj_d, 2 * img, (void*)r->stream, user)))
+          return fail(ESB_ERR_CUDA, std::string(where) + ": the all-reduce callback returned " + std::to_string(rc));
+        if ((rc = esb_rec_compare(r, vg, projections + (size_t)index * img, index))) return rc;
+        ESB_CK(cudaMemcpyAsync(r->sirt_d[i], r->proj_d, img * sizeof(float), cudaMemcpyDeviceToDevice, r->stream),
+               where);
+      }
+      for (int i = 0; i < sirt_count; ++i) {
+        if (s * sirt_count + i >= proj_count) continue;
+        *volume_is_empty = 0;
+        const int index = index_list[s * sirt_count + i];
+        if ((rc = rec_back_project_image(r, vg, vol, voxel_type, index, (float)sirt_count, r->sirt_d[i]))) return rc;
+      }
+    }
   }
   return ok();
 }

@@ -2,18 +2,22 @@
 
 One process per GPU with torch.distributed for the plumbing.
 
-* ``ZSlabSart``: the reference's MPI scheme for one tomogram larger than one
-  GPU (Volume(dim, count, part), Volume.cpp:82-114; EmSart.cpp:579-675 with
-  the projections summed over ranks). Rank r holds z-slab r of the volume.
+* ``Reconstructor.sart_zslab`` with ``torch_allreduce``: the reference's MPI
+  scheme for one tomogram larger than one GPU (Volume(dim, count, part),
+  Volume.cpp:82-114; EmSart.cpp:579-675 with the projections summed over
+  ranks) inside the library (esb_sart_run_zslab): one all-reduce of the
+  slab's projection and ray lengths per projection, on the reconstructor's
+  stream. ``ZSlabSart`` is the same loop in Python over an adapter, which
+  runs it on the CPU oracle in the tests. Rank r holds z-slab r of the volume.
   For every projection each rank forward-projects its slab (line integrals
   and ray lengths through the slab), the projection and the ray-length image
   are summed over ranks with one all-reduce, every rank forms the same
   residual and back-projects it into its own slab. With CTF the slab images
   of each rank are filtered before the sum, which is the same as filtering
   the sum: the filter is linear.
-* ``shard_particles``: EmSartSubVolumes' particles split over ranks
-  (EmSartSubVolumes.cpp:614-668); the projections are replicated and no
-  collective is needed.
+* ``batch_particles``: EmSartSubVolumes' particles split over ranks
+  (EmSartSubVolumes.cpp:611-668), used by reconstruct.reconstruct_subvolumes;
+  the projections are replicated and no collective is needed.
 
 The driver talks to a reconstructor through a small adapter, so the same
 loop runs on the GPU library (``GpuSlab``) and, for tests without a GPU, on
@@ -98,7 +102,42 @@ class ZSlabSart:
         return volume_is_empty
 
 
+def torch_allreduce(group=None):
+    """The all-reduce callback of Reconstructor.sart_zslab over
+    torch.distributed: the sum is enqueued on the reconstructor's stream
+    (NCCL: no host synchronisation; gloo reduces CUDA tensors through the
+    host)."""
+
+    def allreduce(buf, stream):
+        import torch
+        import torch.distributed as dist
+
+        if not dist.is_initialized() or dist.get_world_size(group) == 1:
+            return
+        with torch.cuda.stream(stream):
+            dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+
+    return allreduce
+
+
+def batch_particles(n_particles: int, batch_size: int, rank: int, world: int) -> list[list[int]]:
+    """This rank's particles, batch by batch (EmSartSubVolumes.cpp:611-668):
+    the motive list in batches of batch_size; in each batch rank r takes
+    batch + r, batch + r + world, ... With batch_size a multiple of world
+    this is the reference's split exactly. Otherwise the reference's
+    index batch + pInBatch + rank runs past the batch end into the next batch
+    (and past its per-batch box array), so those particles would be done
+    twice; here every rank stops at its batch's end and each particle is
+    reconstructed once."""
+    if batch_size < 1 or world < 1 or not 0 <= rank < world:
+        raise ValueError("batch_particles: invalid batch size, rank or world size")
+    out = []
+    for b0 in range(0, n_particles, batch_size):
+        end = min(b0 + batch_size, n_particles)
+        out.append(list(range(b0 + rank, end, world)))
+    return out
+
+
 def shard_particles(n_particles: int, rank: int, world: int) -> list[int]:
-    """Particles of this rank: round-robin over ranks, as the reference
-    splits each batch (EmSartSubVolumes.cpp:614-668)."""
-    return [p for p in range(n_particles) if p % world == rank]
+    """All particles of this rank (batch_particles with one batch)."""
+    return batch_particles(n_particles, max(1, n_particles), rank, world)[0] if n_particles else []

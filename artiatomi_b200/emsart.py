@@ -523,6 +523,42 @@ class Reconstructor:
                                il.size, iterations, sirt_count, C.byref(empty)))
         return bool(empty.value)
 
+    def sart_zslab(self, vg, vol, projections, index_list, iterations: int, sirt_count: int, allreduce,
+                   volume_is_empty: bool = True):
+        """esb_sart_run_zslab: SART over this rank's z-slab (vg from
+        volume_geometry(dims, subvol_count=ranks, subvol=rank)). `allreduce`
+        is called once per projection as allreduce(buffer, stream): buffer a
+        torch view of the slab's projection and ray lengths (2 x H x W,
+        contiguous) to be summed over the ranks in place, stream the
+        reconstructor's (a torch.cuda.ExternalStream) on which the sum must be
+        ordered. Returns the updated volume_is_empty flag."""
+        il = np.ascontiguousarray(np.asarray(index_list, np.int32))
+        empty = C.c_int(int(volume_is_empty))
+        H, W = self.cfg.proj_y, self.cfg.proj_x
+        errors = []
+
+        def cb(buf, count, stream, user):
+            import torch
+
+            try:
+                assert count == 2 * H * W
+                # stream NULL: the reconstructor runs on the default stream
+                st = torch.cuda.ExternalStream(stream) if stream else torch.cuda.default_stream()
+                allreduce(device_view(buf, (2, H, W)), st)
+                return 0
+            except Exception as e:  # reported after the call returns
+                errors.append(e)
+                return 1
+
+        fn = L.ALLREDUCE_FN(cb)
+        rc = lib.esb_sart_run_zslab(self._h, C.byref(vg), fptr(vol), _voxel_type_of(vol), fptr(projections),
+                                    fptr(il), il.size, iterations, sirt_count, C.byref(empty), C.cast(fn, C.c_void_p),
+                                    None)
+        if errors:
+            raise errors[0]
+        check(rc)
+        return bool(empty.value)
+
     def subvolume_wbp(self, full_vg, sub_geoms, pair_geoms, boxes, projections, index_list, active=None,
                       batched: bool = True):
         n = len(boxes)

@@ -42,12 +42,31 @@ class _Run:
     H: int
 
 
-def _setup(cfg: EmSartConfig, variant: int) -> _Run:
+def _rank_world(rank, world):
+    """This process's rank and the number of ranks: the arguments, else
+    torch.distributed's when it is initialised, else one rank."""
+    if rank is not None and world is not None:
+        return int(rank), int(world)
+    try:
+        import torch.distributed as dist
+
+        if dist.is_available() and dist.is_initialized():
+            return dist.get_rank(), dist.get_world_size()
+    except ImportError:
+        pass
+    return 0, 1
+
+
+def _setup(cfg: EmSartConfig, variant: int, rank: int = 0) -> _Run:
     """Files in, geometry, reconstructor and the prepared projections
-    (EmSart.cpp / EmSartSubVolumes.cpp up to the reconstruction loop)."""
+    (EmSart.cpp / EmSartSubVolumes.cpp up to the reconstruction loop). Rank r
+    runs on CudaDeviceID[r] (the reference's CudaDeviceIDs[mpi_offset +
+    mpi_host_rank], EmSartSubVolumes.cpp:297-299, on one node), on device r
+    when the list is shorter."""
     import torch
 
-    dev = torch.device("cuda", cfg.CudaDeviceID[0] if cfg.CudaDeviceID else 0)
+    ids = list(cfg.CudaDeviceID or [])
+    dev = torch.device("cuda", ids[rank] if rank < len(ids) else rank)
     torch.cuda.set_device(dev)
     stack, pixel_nm = F.read_stack(cfg.ProjectionFile)
     if stack.dtype not in _PIX:
@@ -139,43 +158,69 @@ def _negated(vol, dev):
     return neg.cpu().numpy()
 
 
+@dataclass
+class SubvolumeBatch:
+    """One batch of EmSartSubVolumes' particle loop on one rank."""
+    parts: list  # motive-list indices of this rank's particles
+    sub: list  # VolGeom of each particle's box
+    pair: object  # ProjGeom[len(parts) * n_proj]: detector frames with the particle's extra shift
+    active: np.ndarray  # [particle][projection]: |extra shift| < MaxShift - 0.5
+
+
+def subvolume_batches(cfg: EmSartConfig, markers, tc, vg, W: int, H: int, rank: int = 0, world: int = 1):
+    """The host side of EmSartSubVolumes' particle loop
+    (EmSartSubVolumes.cpp:611-668) for one rank: the motive list in batches of
+    BatchSize, each batch split over the ranks (distributed.batch_particles),
+    and per particle its box placement (Volume::PositionInSpace) and the
+    detector frames with its extra shifts. No device work."""
+    from .distributed import batch_particles
+
+    motl = F.read_motive_list(cfg.MotiveList, cfg.ScaleMotivelistPosition, cfg.ScaleMotivelistShift)
+    shifts = F.read_shift_file(cfg.ShiftInputFile)  # [projection][motive][2]
+    n_proj = len(markers.tilt_angle)
+    out = []
+    for parts in batch_particles(motl.shape[0], max(1, cfg.BatchSize), rank, world):
+        sub = []
+        pair = (L.ProjGeom * (len(parts) * n_proj))()
+        active = np.zeros((len(parts), n_proj), np.uint8)
+        for k, p in enumerate(parts):
+            m = motl[p]
+            sub.append(E.subvolume_geometry(cfg.SizeSubVol, cfg.VoxelSizeSubVol, vg, m[7:10], m[10:13]))
+            es = shifts[:, p, :]  # [projection][2]
+            g = E.projection_geometry(markers, W, H, tc, extra_shift=es)
+            for i in range(n_proj):
+                pair[k * n_proj + i] = g[i]
+            active[k] = np.sqrt((es.astype(np.float32) ** 2).sum(1)) < np.float32(cfg.MaxShift - 0.5)
+        out.append(SubvolumeBatch(parts, sub, pair, active))
+    return out
+
+
 def reconstruct_subvolumes(cfg: EmSartConfig, write: bool = True, batched: bool = True,
-                           variant: int = E.VARIANT_FAST):
+                           variant: int = E.VARIANT_FAST, rank: int | None = None, world: int | None = None):
     """EmSartSubVolumes' run (EmSartSubVolumes.cpp:611-705): weighted
     back-projection of a SizeSubVol^3 box around every particle of the motive
     list, each projection shifted by the particle's extra shift from the
     shift file (tilts with |shift| >= MaxShift - 0.5 are left out), BatchSize
     particles per pass, every box written negated to
-    SubVolPath + <particle index coding> + ".em". Returns {file name: box}."""
+    SubVolPath + <particle index coding> + ".em". With several ranks (the
+    arguments, or torch.distributed's) each batch is split over them as the
+    reference's MPI run splits it; the projections are replicated and no
+    collective is needed. Returns {file name: box} of this rank's
+    particles."""
     import torch
 
-    R = _setup(cfg, variant)
+    rank, world = _rank_world(rank, world)
+    R = _setup(cfg, variant, rank)
     rec, vg, dev = R.rec, R.vg, R.dev
     motl = F.read_motive_list(cfg.MotiveList, cfg.ScaleMotivelistPosition, cfg.ScaleMotivelistShift)
-    shifts = F.read_shift_file(cfg.ShiftInputFile)  # [projection][motive][2]
-    n_part = motl.shape[0]
-    n_proj = len(R.tilt)
     index_list = E.projection_index_list(E.PLT_NORMAL, R.tilt, R.good.astype(np.int32))
-    batch = max(1, cfg.BatchSize)
     S = cfg.SizeSubVol
     out = {}
-    for b0 in range(0, n_part, batch):
-        parts = list(range(b0, min(b0 + batch, n_part)))
-        sub, boxes = [], []
-        pair = (L.ProjGeom * (len(parts) * n_proj))()
-        active = np.zeros((len(parts), n_proj), np.uint8)
-        for k, p in enumerate(parts):
-            m = motl[p]
-            sub.append(E.subvolume_geometry(S, cfg.VoxelSizeSubVol, vg, m[7:10], m[10:13]))
-            es = shifts[:, p, :]  # [projection][2]
-            g = E.projection_geometry(R.markers, R.W, R.H, R.tc, extra_shift=es)
-            for i in range(n_proj):
-                pair[k * n_proj + i] = g[i]
-            active[k] = np.sqrt((es.astype(np.float32) ** 2).sum(1)) < np.float32(cfg.MaxShift - 0.5)
-            boxes.append(torch.zeros((S, S, S), dtype=torch.float32, device=dev))
-        rec.subvolume_wbp(vg, sub, pair, boxes, R.prepared, index_list, active=active, batched=batched)
+    for b in subvolume_batches(cfg, R.markers, R.tc, vg, R.W, R.H, rank, world):
+        boxes = [torch.zeros((S, S, S), dtype=torch.float32, device=dev) for _ in b.parts]
+        rec.subvolume_wbp(vg, b.sub, b.pair, boxes, R.prepared, index_list, active=b.active, batched=batched)
         torch.cuda.synchronize()
-        for k, p in enumerate(parts):
+        for k, p in enumerate(b.parts):
             name = cfg.SubVolPath + F.index_coding(motl[p], cfg.NamingConvention == 1) + ".em"
             box = _negated(boxes[k], dev)
             out[name] = box

@@ -487,6 +487,30 @@ int esb_subvolume_wbp(esb_reconstructor* rec, const esb_vol_geom* full_vol, int 
                       float* const* boxes, const float* projections, const int* index_list, int proj_count,
                       int batched);
 
+/* The collective of a z-slab SART: sums `count` floats at device address
+ * `buf` over the ranks, in place, ordered on `stream` (for example
+ * ncclAllReduce(buf, buf, count, ncclFloat, ncclSum, comm, stream), or a
+ * host-side reduction that synchronises the stream first); returns 0 on
+ * success. */
+typedef int (*esb_allreduce_fn)(float* buf, size_t count, void* stream, void* user);
+
+/* EmSart.cpp:579-675 over one z-slab of the volume per rank, the reference's
+ * MPI decomposition (Volume(dim, count, part), Volume.cpp:82-114; vg from
+ * esb_volume_geometry(dim, ranks, rank, ...), vol the slab's voxels). For
+ * every projection the slab's forward projection and ray lengths (one
+ * contiguous buffer of 2 x W x H floats: projection, then ray lengths) are
+ * summed over the ranks with ONE call of `allreduce`, enqueued on the
+ * reconstructor's stream between the forward projection and the compare
+ * with no host synchronisation; every rank then forms the same residual
+ * and back-projects it into its slab. (The reference gathers both images on
+ * rank 0, Reconstructor.cpp:440-463, and broadcasts the residuals,
+ * EmSart.cpp:647.) With CTF each rank filters its own slab images before the
+ * sum, which equals filtering the sum. Every rank calls it with the same
+ * arguments, so the collectives match in order. */
+int esb_sart_run_zslab(esb_reconstructor* rec, const esb_vol_geom* vg, void* vol, int voxel_type,
+                       const float* projections, const int* index_list, int proj_count, int iterations, int sirt_count,
+                       int* volume_is_empty, esb_allreduce_fn allreduce, void* user);
+
 /* ------------------------------------------------ no-allocation variant
  * No counterpart in the reference. One SART update of `vol` from one
  * projection without CTF: the sequence esb_rec_reset_projections,

@@ -4,10 +4,14 @@ particle sharding of the sub-volume reconstruction.
 World size 2 over gloo on 127.0.0.1. The CPU tests run the driver of
 artiatomi_b200.distributed on the oracle (one slab per process) and check it
 against the same decomposition emulated in one process, bit for bit (the
-all-reduce of two float images is one float addition per pixel). The GPU
-test runs two processes on the one GPU with gloo (host-side reduction: no
-kernel waits on another process) and checks them against the same
-decomposition run in one process on the GPU.
+all-reduce of two float images is one float addition per pixel), and run
+the particle split of reconstruct.subvolume_batches on two ranks, each
+back-projecting its particles on the oracle, against the one-rank run. The
+GPU test runs the library's z-slab SART (Reconstructor.sart_zslab, the C
+entry esb_sart_run_zslab with a torch.distributed all-reduce callback) in two
+processes on the one GPU with gloo (host-side reduction: no kernel waits on
+another process) and checks them against the same decomposition run in one
+process on the GPU.
 """
 import os
 import socket
@@ -160,12 +164,162 @@ def test_zslab_sart_two_ranks_matches_emulation():
 
 
 def test_particle_shards_cover_every_particle_once():
-    from artiatomi_b200.distributed import shard_particles
+    from artiatomi_b200.distributed import batch_particles, shard_particles
 
-    for n, world in ((7, 2), (10, 3), (1, 4)):
+    for n, world in ((7, 2), (10, 3), (1, 4), (0, 2)):
         parts = [shard_particles(n, r, world) for r in range(world)]
         flat = sorted(p for ps in parts for p in ps)
         assert flat == list(range(n))
+    for n, batch, world in ((11, 4, 2), (9, 6, 3), (5, 3, 2), (3, 8, 4), (6, 1, 1)):
+        per_rank = [batch_particles(n, batch, r, world) for r in range(world)]
+        assert all(len(b) == (n + batch - 1) // batch for b in per_rank)
+        flat = sorted(p for b in per_rank for ps in b for p in ps)
+        assert flat == list(range(n))
+        for r in range(world):
+            for k, ps in enumerate(per_rank[r]):
+                b0 = k * batch
+                assert all(b0 <= p < b0 + batch for p in ps)
+                if batch % world == 0:
+                    # the reference's motlIdx = batch + pInBatch + mpi_part
+                    ref = [b0 + q + r for q in range(0, batch, world) if b0 + q + r < n]
+                    assert ps == ref
+    with pytest.raises(ValueError):
+        batch_particles(4, 2, 2, 2)
+
+
+# -- particle-sharded sub-volumes -------------------------------------------
+
+SUB_N, SUB_S = 7, 12
+
+
+def _write_subvolume_dataset(d):
+    """tilt series, markers, motive list, shift file and config of a small
+    EmSartSubVolumes run; returns the oracle-prepared projections."""
+    from pathlib import Path
+
+    from tests.test_reconstruct import H as RH
+    from tests.test_reconstruct import N as NP
+    from tests.test_reconstruct import W as RW
+    from tests.test_reconstruct import _dataset
+    from artiatomi_b200 import fileio as F
+    from artiatomi_b200.config import EmSartConfig
+    from oracle.driver import prepare_projection
+
+    d = Path(d)
+    raw, tilt, psi, og, vo = _dataset(d, wbp=True)
+    rng = np.random.default_rng(13)
+    motl = np.zeros((SUB_N, 20), np.float32)
+    motl[:, 3] = np.arange(1, SUB_N + 1)
+    motl[:, 7:10] = np.stack([rng.uniform(18, 46, SUB_N), rng.uniform(18, 46, SUB_N), rng.uniform(8, 16, SUB_N)], 1)
+    motl[:, 10:13] = rng.uniform(-1, 1, (SUB_N, 3))
+    F.write_motive_list(str(d / "motl.em"), motl)
+    F.write_shift_file(str(d / "shifts.em"), rng.uniform(-1.8, 1.8, (2, NP, SUB_N)).astype(np.float32))
+    (d / "sub").mkdir(exist_ok=True)
+    text = (d / "emsart.cfg").read_text() + f"""SizeSubVol = {SUB_S}
+VoxelSizeSubVol = 1
+MotiveList = {d / 'motl.em'}
+SubVolPath = {d / 'sub'}/
+ShiftInputFile = {d / 'shifts.em'}
+BatchSize = 4
+MaxShift = 2
+ScaleMotivelistShift = 1
+ScaleMotivelistPosition = 1
+"""
+    (d / "emsart_sub.cfg").write_text(text)
+    cfg = EmSartConfig.from_text(text, subvolumes=True)
+    pc = dict(wbp=1, normalization=cfg.ProjectionNormalization, correct_bad_pixels=1,
+              bad_pixel_value=cfg.BadPixelValue, skip_filter=int(cfg.SkipFilter), lp=float(cfg.fourFilterLP),
+              hp=float(cfg.fourFilterHP), lps=float(cfg.fourFilterLPS), hps=float(cfg.fourFilterHPS),
+              wbp_filter=cfg.WBPFilter)
+    prepared = np.stack([prepare_projection(raw[i], max(RW, RH), dict(pc, tilt_deg=float(tilt[i]),
+                                                                      psi_deg=float(psi[i])))[0]
+                         for i in range(NP)])
+    np.save(d / "prepared.npy", prepared)
+
+
+def _oracle_vg(v):
+    from oracle import geometry as G
+
+    a = lambda x: np.asarray(list(x), np.float32)  # noqa: E731
+    return G.VolGeom(a(v.bbox_min), a(v.bbox_max), a(v.bbox_rcp), a(v.dim), a(v.voxel_size), float(v.z_shift),
+                     a(v.full_dim), a(v.full_bbox_min), a(v.full_bbox_max))
+
+
+def _subvolumes_on_oracle(d, rank, world):
+    """reconstruct_subvolumes' batches for this rank, each particle box
+    back-projected by the oracle from the library's own geometry."""
+    from pathlib import Path
+
+    import artiatomi_b200 as E
+    from artiatomi_b200 import fileio as F
+    from artiatomi_b200.config import EmSartConfig
+    from artiatomi_b200.reconstruct import _rank_world, subvolume_batches
+    from oracle.driver import OracleReconstructor
+    from tests.test_reconstruct import H as RH
+    from tests.test_reconstruct import W as RW
+
+    d = Path(d)
+    rank, world = _rank_world(rank, world)
+    cfg = EmSartConfig.from_text((d / "emsart_sub.cfg").read_text(), subvolumes=True)
+    md = F.read_markers(cfg.MarkerFile, cfg.ReferenceMarker)
+    markers = md.markers()
+    tc = E.TiltConfig(cfg.AddTiltAngle, cfg.AddTiltXAngle, cfg.UseFixPsiAngle, cfg.PsiAngle, cfg.PhiAngle)
+    vg = E.volume_geometry(cfg.RecDimensions, cfg.VoxelSize, cfg.VolumeShift)
+    n_proj = len(markers.tilt_angle)
+    prepared = np.load(d / "prepared.npy")
+    orc = OracleReconstructor(dict(lambda_=cfg.Lambda, oversampling=cfg.OverSampling, cut_length=cfg.CutLength,
+                                   dim_length=cfg.DimLength), RW, RH, None, markers.tilt_angle, precision=1)
+    il = E.projection_index_list(E.PLT_NORMAL, markers.tilt_angle)
+    boxes, batches = {}, []
+    for b in subvolume_batches(cfg, markers, tc, vg, RW, RH, rank, world):
+        batches.append(list(b.parts))
+        pair = [[{"det": list(g.detektor), "u": list(g.u_pitch), "v": list(g.v_pitch), "n": list(g.proj_norm),
+                  "detMat": list(g.detector_matrix)} for g in b.pair[k * n_proj:(k + 1) * n_proj]]
+                for k in range(len(b.parts))]
+        bo = [np.zeros((SUB_S,) * 3, np.float32) for _ in b.parts]
+        orc.subvolume_wbp(_oracle_vg(vg), [_oracle_vg(v) for v in b.sub], pair, bo, prepared, il, active=b.active)
+        for k, p in enumerate(b.parts):
+            boxes[p] = bo[k]
+    return boxes, batches
+
+
+def _worker_subvolumes(rank, world, port, d):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        boxes, batches = _subvolumes_on_oracle(d, None, None)  # rank and world from torch.distributed
+        np.savez(os.path.join(d, f"boxes{rank}.npz"), batches=np.array(repr(batches)),
+                 **{f"p{p}": b for p, b in boxes.items()})
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_reconstruct_subvolumes_particle_sharding_two_ranks():
+    import torch.multiprocessing as mp
+
+    with tempfile.TemporaryDirectory() as d:
+        _write_subvolume_dataset(d)
+        mp.spawn(_worker_subvolumes, args=(2, _free_port(), d), nprocs=2, join=True)
+        got = [np.load(os.path.join(d, f"boxes{r}.npz")) for r in range(2)]
+        single, single_batches = _subvolumes_on_oracle(d, 0, 1)
+    # BatchSize 4 over 2 ranks: the reference's split within each batch
+    assert eval(str(got[0]["batches"])) == [[0, 2], [4, 6]]
+    assert eval(str(got[1]["batches"])) == [[1, 3], [5]]
+    assert single_batches == [[0, 1, 2, 3], [4, 5, 6]]
+    seen = []
+    for g in got:
+        for key in g.files:
+            if key == "batches":
+                continue
+            p = int(key[1:])
+            seen.append(p)
+            assert np.abs(single[p]).max() > 0
+            np.testing.assert_array_equal(g[key], single[p])
+    assert sorted(seen) == list(range(SUB_N))
 
 
 def _worker_gpu(rank, world, port, outdir):
@@ -173,7 +327,7 @@ def _worker_gpu(rank, world, port, outdir):
     import torch.distributed as dist
 
     import artiatomi_b200 as E
-    from artiatomi_b200.distributed import GpuSlab, ZSlabSart
+    from artiatomi_b200.distributed import torch_allreduce
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -185,7 +339,9 @@ def _worker_gpu(rank, world, port, outdir):
         vg = E.volume_geometry(DIMS, subvol_count=world, subvol=rank)
         vol = torch.zeros((int(vg.dim[2]), DIMS[1], DIMS[0]), device="cuda")
         rec = E.Reconstructor(E.ReconConfig(W, H, N_PROJ, variant=E.VARIANT_FAST, **CFG), case["pg"], case["tilt"])
-        ZSlabSart(GpuSlab(rec, vg, vol)).run(projs, il, iterations=2, sirt_count=2)
+        empty = rec.sart_zslab(vg, vol, projs, il, 2, 2, torch_allreduce())
+        assert not empty
+        torch.cuda.synchronize()
         np.save(os.path.join(outdir, f"slab{rank}.npy"), vol.cpu().numpy())
         rec.close()
     finally:
