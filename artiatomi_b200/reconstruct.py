@@ -40,6 +40,7 @@ class _Run:
     dev: object
     W: int
     H: int
+    mag_inv: np.ndarray  # the inverse magnification anisotropy, 3 x 3 row-major
 
 
 def _rank_world(rank, world):
@@ -81,7 +82,8 @@ def _setup(cfg: EmSartConfig, variant: int, rank: int = 0) -> _Run:
     vg = E.volume_geometry(cfg.RecDimensions, cfg.VoxelSize, cfg.VolumeShift)
     amount, angle = cfg.MagAnisotropy
     mag = E.mag_aniso_matrix(amount, angle, W, H)
-    mag_inv = E.mag_aniso_matrix(1.0 / amount, angle, W, H)
+    # GetMagAnistropyMatrix(1.0f / amount, ...): the reciprocal in float
+    mag_inv = E.mag_aniso_matrix(float(np.float32(1.0) / np.float32(amount)), angle, W, H)
     defocus = F.read_ctf(cfg.CtfFile).ravel() if cfg.CtfMode else None
     rc = E.ReconConfig(W, H, n, lambda_=cfg.Lambda, oversampling=cfg.OverSampling, ctf_mode=cfg.CtfMode,
                        cut_length=cfg.CutLength, dim_length=cfg.DimLength, crop=cfg.Crop, crop_dim=cfg.CropDim,
@@ -113,7 +115,7 @@ def _setup(cfg: EmSartConfig, variant: int, rank: int = 0) -> _Run:
                   tilt_deg=float(tilt[i]), psi_deg=float(psi[i] if psi is not None else 0.0),
                   wbp_filter=cfg.WBPFilter)
         stats.append(rec.prepare_projection(raw, prepared[i], **pc))
-    return _Run(rec, pg, vg, markers, tilt, good, prepared, stats, pixel_nm, tc, dev, W, H)
+    return _Run(rec, pg, vg, markers, tilt, good, prepared, stats, pixel_nm, tc, dev, W, H, mag_inv)
 
 
 def reconstruct(cfg: EmSartConfig, write: bool = True, variant: int = E.VARIANT_FAST, graphs: bool = True):

@@ -48,16 +48,50 @@ from .config import EmSartConfig
 from .reconstruct import _setup
 
 
-def _particle_roi(c, m, vg, vs, safe, W, H):
-    """Detector region around the particle centre (Projection::ComputeHitPoint
-    of the voxel centre, widened by the reference's safeDist)."""
-    bmin = np.array(vg.bbox_min[:], np.float64)
-    p = bmin + (m[7:10].astype(np.float64) + m[10:13] - 1.0) * vs + 0.5 * vs
-    M = np.array(c.detector_matrix[:], np.float64).reshape(4, 4)
-    u = M[0, :3] @ p + M[0, 3]
-    v = M[1, :3] @ p + M[1, 3]
-    return (max(int(math.floor(u)) - safe, 0), max(int(math.floor(v)) - safe, 0),
-            min(int(math.ceil(u)) + safe, W), min(int(math.ceil(v)) + safe, H))
+def hit_point(pg, x, y, z):
+    """Projection::ComputeHitPoint (Projection.cpp:1051-1085) in float32: the
+    foot of the normal from (x, y, z) on projection pg's detector plane,
+    through its detector matrix (GetDetectorMatrix with os 1), each pixel
+    coordinate truncated to int as the reference assigns it to an int2."""
+    f = np.float32
+    p = [f(x), f(y), f(z)]
+    d = [f(a) for a in pg.detektor]
+    n = [f(a) for a in pg.proj_norm]
+    t = (n[0] * p[0] + n[1] * p[1]) + n[2] * p[2]
+    t = t + (((-n[0]) * d[0] - n[1] * d[1]) - n[2] * d[2])
+    t = abs(t)
+    h = [t * (-n[k]) + p[k] for k in range(3)]
+    M = [f(a) for a in pg.detector_matrix]
+    u = ((M[0] * h[0] + M[1] * h[1]) + M[2] * h[2]) + f(1) * M[3]
+    v = ((M[4] * h[0] + M[5] * h[1]) + M[6] * h[2]) + f(1) * M[7]
+    return int(u), int(v)
+
+
+def safe_dist(cfg: EmSartConfig) -> int:
+    """EmSartRefine's safeDist, 100 + VoxelSizeSubVol * SizeSubVol * 2 +
+    MaxShift * 2 evaluated in float and truncated (EmSartRefine.cpp:830)."""
+    f = np.float32
+    return int(f(100) + f(cfg.VoxelSizeSubVol) * f(cfg.SizeSubVol) * f(2) + f(int(cfg.MaxShift) * 2))
+
+
+def particle_roi(pg, m, vg, vs, safe, mag_inv):
+    """A particle's detector region as EmSartRefine.cpp:815-847 forms it:
+    the hit point of the particle centre (bbMin + (coord + shift - 1) * vs +
+    vs / 2, in float), as ints, through the inverse magnification anisotropy
+    (MatrixVector3Mul of the 3 x 3 matrix on (x, y, 1)), then
+    floor - safeDist .. ceil + safeDist; the minima clamped at 0, the maxima
+    not (the projection kernels clip them to the detector). Returns
+    (x_min, y_min, x_max, y_max)."""
+    f = np.float32
+    bmin = [f(a) for a in vg.bbox_min]
+    vs = [f(a) for a in vs]
+    c = [(bmin[k] + ((f(m[7 + k]) + f(m[10 + k])) - f(1)) * vs[k]) + f(0.5) * vs[k] for k in range(3)]
+    hx, hy = hit_point(pg, *c)
+    A = [f(a) for a in np.asarray(mag_inv, np.float32).ravel()]
+    x = (A[0] * f(hx) + A[1] * f(hy)) + A[2] * f(1)
+    y = (A[3] * f(hx) + A[4] * f(hy)) + A[5] * f(1)
+    return (max(int(math.floor(x)) - safe, 0), max(int(math.floor(y)) - safe, 0),
+            int(math.ceil(x)) + safe, int(math.ceil(y)) + safe)
 
 
 def _fit_shift(c_sub, ref, target, roi, iterations, max_shift, out):
@@ -291,8 +325,8 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
         raise ValueError("every supporting reference needs its supporting motive list")
     n_part, n_proj = motl.shape[0], len(R.tilt)
     index_list = E.projection_index_list(E.PLT_NORMAL, R.tilt, R.good.astype(np.int32))
-    vs = np.array(cfg.VoxelSize, np.float64)
-    safe = int(100 + cfg.VoxelSizeSubVol * S * 2 + cfg.MaxShift * 2)  # EmSartRefine's safeDist
+    vs = np.array(cfg.VoxelSize, np.float32)
+    safe = safe_dist(cfg)
     extra = np.zeros((n_proj, n_part, 2), np.float32)
     max_shift = int(cfg.MaxShift)
     multi = bool(cfg.MultiPeakDetection)
@@ -338,19 +372,19 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
             i = int(i)
             c_full = E.set_constant_values(R.pg[i], vg)
             # the model: every particle projected over its own region; the
-            # reconstruction over the union of the regions
+            # reconstruction over the union of the regions, which starts as
+            # (W, H)..(0, 0) (EmSartRefine.cpp:799-800, 838-847)
             x0, y0, x1, y1 = W, H, 0, 0
             parts_roi = []
             for m, rot, sub in parts:
-                r = _particle_roi(c_full, m, vg, vs, safe, W, H)
-                if r[2] <= r[0] or r[3] <= r[1]:
-                    continue
+                r = particle_roi(R.pg[i], m, vg, vs, safe, R.mag_inv)
                 x0, y0, x1, y1 = min(x0, r[0]), min(y0, r[1]), max(x1, r[2]), max(y1, r[3])
                 parts_roi.append((sub, rot, r))
-            if x1 <= x0 or y1 <= y0:
-                continue
-            roi = (x0, y0, x1, y1)
+            roi = (x0, y0, min(x1, W), min(y1, H))
             if method == "cc":
+                # an empty union is measured as the reference measures it:
+                # nothing is projected, GetDisplacement of the images as they
+                # are (no positive correlation: the shift (-1000, -1000))
                 sx, sy, cc_value = _cc_shift(R, vg, i, vol, parts_roi, roi, bufs, max_shift, multi, (cmap, cmulti))
                 shift = np.array([-sx, -sy], np.float32)  # the file holds the shift; the extra shift is its negation
                 if dump:
@@ -358,6 +392,8 @@ def refine_shifts(cfg: EmSartConfig, write: bool = True, iterations: int = 10, p
                     if multi:
                         cc_multi.setdefault(i, []).append(cmulti.cpu().numpy().copy())
             else:
+                if roi[2] <= roi[0] or roi[3] <= roi[1]:
+                    continue
                 m, rot, sub = parts[0]
                 proj.zero_()
                 E.forward_project(c_full, vol, proj, dist, roi=roi, fast=True)

@@ -454,3 +454,62 @@ def test_relations_text_format(tmp_path):
     rel = np.array([[12, 3, 7, 0], [0, 0, 0, 0], [5, 9, 1, 4]])
     write_relations(str(tmp_path / "r"), rel, np.array([0.8125, 0.0, 1.0e-5], np.float32))
     assert (tmp_path / "r").read_text() == "12; 3; 3; 0; 0.8125\n0; 0; 0; 0; 0\n5; 9; 9; 4; 1e-05\n"
+
+
+def test_particle_region_with_magnification_anisotropy():
+    """EmSartRefine.cpp:815-847: the particle centre's hit point truncated to
+    whole pixels, through the inverse anisotropy matrix, then floor / ceil
+    -+ safeDist (minima clamped at 0). Checked against the same steps done by
+    hand in double: the hit point solved on the detector plane from the
+    pixel pitches, the 3 x 3 matrix applied to (x, y, 1). Cases whose hand
+    values fall within 1e-3 of a whole pixel are skipped (float and double
+    may round them apart)."""
+    import math
+
+    import artiatomi_b200 as E
+    from types import SimpleNamespace
+
+    from artiatomi_b200.refine import particle_roi, safe_dist
+
+    W = H = 512
+    n = 7
+    rng = np.random.default_rng(3)
+    tilt = np.linspace(-54.0, 54.0, n).astype(np.float32)
+    m = E.Markers(tilt, rng.uniform(-3, 3, n).astype(np.float32), rng.uniform(-3, 3, n).astype(np.float32),
+                  np.ones(n, np.float32), np.full(n, 4.0, np.float32))
+    pg = E.projection_geometry(m, W, H, E.TiltConfig(0.0, 0.0, False, 0.0, 0.0))
+    vs = (2.0, 2.0, 2.0)
+    vg = E.volume_geometry((256, 256, 96), vs, (0.0, 0.0, 0.0))
+    safe = safe_dist(SimpleNamespace(SizeSubVol=24, VoxelSizeSubVol=1.5, MaxShift=7))
+    assert safe == 100 + 72 + 14
+    inv = E.mag_aniso_matrix(float(np.float32(1) / np.float32(1.04)), 35.0, W, H)
+    ident = E.mag_aniso_matrix(1.0, 35.0, W, H)
+    A = np.asarray(inv, np.float64).reshape(3, 3)
+    checked = moved = 0
+    for i in range(n):
+        g = pg[i]
+        det, n_ = np.array(g.detektor, np.float64), np.array(g.proj_norm, np.float64)
+        P = np.stack([np.array(g.u_pitch, np.float64), np.array(g.v_pitch, np.float64)], 1)
+        for _ in range(6):
+            mot = np.zeros(20, np.float32)
+            mot[7:10] = rng.uniform([20, 20, 10], [236, 236, 86])
+            mot[10:13] = rng.uniform(-2, 2, 3)
+            c = np.array(vg.bbox_min, np.float64) + (mot[7:10].astype(np.float64) + mot[10:13] - 1.0) * 2.0 + 1.0
+            t = abs(n_ @ (c - det))
+            hit = c - t * n_
+            uv = np.linalg.lstsq(P, hit - det, rcond=None)[0]
+            if np.min(np.abs(uv - np.round(uv))) < 1e-3:
+                continue
+            hx, hy = int(uv[0]), int(uv[1])
+            x, y = A[0, 0] * hx + A[0, 1] * hy + A[0, 2], A[1, 0] * hx + A[1, 1] * hy + A[1, 2]
+            if min(abs(x - round(x)), abs(y - round(y))) < 1e-3:
+                continue
+            want = (max(math.floor(x) - safe, 0), max(math.floor(y) - safe, 0), math.ceil(x) + safe,
+                    math.ceil(y) + safe)
+            got = particle_roi(g, mot, vg, vs, safe, inv)
+            assert got == want, (i, got, want)
+            plain = particle_roi(g, mot, vg, vs, safe, ident)
+            moved = max(moved, abs(plain[2] - got[2]), abs(plain[3] - got[3]))
+            checked += 1
+    assert checked >= 30
+    assert moved >= 5  # the anisotropy moves the region by whole pixels
