@@ -116,6 +116,8 @@ _SIGS = {
     "esb_reconstructor_enable_timing": ([P, I], I),
     "esb_reconstructor_timing": ([P, P, P], I),
     "esb_reconstructor_enable_graphs": ([P, I], I),
+    "esb_reconstructor_fuse_subsets": ([P, I], I),
+    "esb_reconstructor_subvolume_patches": ([P, I], I),
     "esb_prepare_projection": ([P, C.POINTER(PrepareConfig), P, P, C.POINTER(F), C.POINTER(F), C.POINTER(I)], I),
     "esb_rec_cc_displacement": ([P, P, P, I, I, P, C.POINTER(F), P, P], I),
     "esb_rec_forward_projection": ([P, C.POINTER(VolGeom), P, I, I, I], I),

@@ -42,6 +42,10 @@ cudaError_t launch_upsample(const KConst& k, const float* imgs, size_t img_strid
                             int linear, float2* up, size_t up_stride, cudaStream_t st);
 bool bp_can_upsample(const KConst& k, int os);
 bool bp_uses_axis(const KConst& k, int os);
+bool bp_set_eligible(const KConst& k, int os, int nslab);
+cudaError_t launch_bp_axis_set(const KConst* ks, const float2* const* ups, const SlabTable* slabs, int count,
+                               size_t up_stride, void* vol, int vt, int pw, int ph, float lambda, int os,
+                               const BpShape* shape, cudaStream_t st);
 cudaError_t launch_slicer_fused(const KConst& c, const void* vol, int vt, float* imgs, size_t img_stride,
                                 size_t pitchE, const SlabTable& slabs, int x0, int y0, int x1, int y1, cudaStream_t st, int nw = 4);
 cudaError_t launch_compare(int pw, int ph, size_t pitchE, const float* real, float* virt, const float* dist,
@@ -456,6 +460,8 @@ struct esb_reconstructor {
   cufftHandle r2c_many[ESB_CTF_SLAB_BATCH + 1] = {};
   bool r2c_many_ok[ESB_CTF_SLAB_BATCH + 1] = {};
   bool graphs = false;                   // replay SART iterations from a captured graph
+  int fuse_subsets = -1;                 // subset back-projection in one volume pass: 1 on, 0 off, -1 half volumes
+  bool subvol_patches = false;           // sub-volume WBP with CTF: all tilts in one launch from gathered patches
   cudaGraphExec_t sart_exec = nullptr;   // the last captured iteration
   // inputs the captured iteration was recorded with (it replays only for the
   // same ones) and the library kernels it launches
@@ -654,6 +660,18 @@ int esb_reconstructor_enable_timing(esb_reconstructor* rec, int enable) {
 int esb_reconstructor_enable_graphs(esb_reconstructor* rec, int enable) {
   if (!rec) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_enable_graphs: NULL reconstructor");
   rec->graphs = enable != 0;
+  return ok();
+}
+
+int esb_reconstructor_fuse_subsets(esb_reconstructor* rec, int enable) {
+  if (!rec) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_fuse_subsets: NULL reconstructor");
+  rec->fuse_subsets = enable < 0 ? -1 : (enable != 0);
+  return ok();
+}
+
+int esb_reconstructor_subvolume_patches(esb_reconstructor* rec, int enable) {
+  if (!rec) return fail(ESB_ERR_INVALID_ARGUMENT, "esb_reconstructor_subvolume_patches: NULL reconstructor");
+  rec->subvol_patches = enable != 0;
   return ok();
 }
 
@@ -1292,6 +1310,95 @@ static int rec_back_project_image(esb_reconstructor* r, const esb_vol_geom* vg, 
   return ESB_OK;
 }
 
+// The back-projections of one ordered subset (EmSart.cpp:649-673) in one
+// pass over the volume per chunk (launch_bp_axis_set): each projection's
+// residual is cropped or CTF-filtered per slab and pre-sampled exactly as
+// rec_back_project_image does it, into its own part of the pre-sampled image
+// buffer; a chunk is as many consecutive projections as fit ESB_BP_SET_MAX and
+// the buffer cap. `done` stays false (nothing launched) when a projection
+// cannot join (faithful kernels, geometry without the single-axis kernel or
+// pre-sampling, too many slabs); the caller then back-projects each one.
+static int rec_back_project_subset(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type,
+                                   const int* indices, int n, float sirt_count, float* const* imgs, bool& done) {
+  done = false;
+  const esb_recon_config& cf = r->cfg;
+  const bool on = r->fuse_subsets > 0 || (r->fuse_subsets < 0 && voxel_type != ESB_VOXEL_F32);
+  if (!on || cf.variant != ESB_VARIANT_FAST || n < 2) return ESB_OK;
+  const int W = cf.proj_x, H = cf.proj_y, os = cf.oversampling;
+  const size_t img = (size_t)W * H, up_stride = (size_t)W * os * (size_t)H * os;
+  const size_t cap_images = std::max<size_t>(1, ((size_t)16 << 30) / (up_stride * sizeof(float2)));
+  std::vector<KConst> ks(n);
+  std::vector<SlabTable> T(n);
+  std::vector<int> cnt(n);
+  int rc;
+  for (int j = 0; j < n; ++j) {
+    ks[j] = rec_const(r, r->geoms[indices[j]], *vg, 1);
+    T[j].count = 0;
+    if (cf.ctf_mode && (rc = rec_slab_table(r, vg, indices[j], T[j]))) return rc;
+    cnt[j] = cf.ctf_mode ? T[j].count : 1;
+    if (!bp_set_eligible(ks[j], os, T[j].count) || (size_t)cnt[j] > cap_images) return ESB_OK;
+  }
+  // chunks of consecutive projections: [first, first + size)
+  std::vector<std::pair<int, int>> chunks;
+  size_t most = 0;
+  for (int j = 0; j < n;) {
+    int m = 0;
+    size_t tot = 0;
+    while (j + m < n && m < ESB_BP_SET_MAX && tot + cnt[j + m] <= cap_images) tot += cnt[j + m++];
+    chunks.emplace_back(j, m);
+    most = std::max(most, tot);
+    j += m;
+  }
+  const size_t need = most * up_stride;
+  if (need > r->up_cap) {
+    ESB_CK(cudaStreamSynchronize(r->stream), "subset back projection");
+    cudaFree(r->up_imgs);
+    r->up_imgs = nullptr;
+    r->up_cap = 0;
+    ESB_CK(cudaMalloc(&r->up_imgs, need * sizeof(float2)), "subset back projection");
+    r->up_cap = need;
+  }
+  done = true;
+  const float lambda = cf.lambda / sirt_count;
+  for (const auto& ch : chunks) {
+    const float2* ups[ESB_BP_SET_MAX];
+    size_t off = 0;
+    for (int j = ch.first; j < ch.first + ch.second; ++j) {
+      const int index = indices[j];
+      int p[8];
+      esb_compute_hit_points(&r->geoms[index], vg, p);
+      float2* up = r->up_imgs + off * up_stride;
+      if (cf.ctf_mode) {
+        if ((rc = rec_slab_capacity(r, T[j].count))) return rc;
+        // cropBorder(proj_d) is re-applied to the residual on every slab (:954)
+        if ((rc = rec_ctf_chain_slabs(r, T[j], index, imgs[j], 1, 1, p, 0, r->slab_imgs, nullptr, 1, p, 1))) return rc;
+        PhaseScope ps(r, 1);
+        ESB_CK(launch_upsample(ks[j], r->slab_imgs, img, T[j].count, W, H, os, 1, up, up_stride, r->stream),
+               "subset back projection");
+      } else {
+        if ((rc = rec_slab_capacity(r, 1))) return rc;
+        PhaseScope ps(r, 3);
+        ESB_CK(launch_crop_border(W, H, W, imgs[j], make_float2(cf.cut_length[0], cf.cut_length[1]),
+                                  make_float2(cf.dim_length[0], cf.dim_length[1]), p, r->stream),
+               "subset back projection");
+        ESB_CK(launch_transpose(imgs[j], W, H, W, r->slab_imgs, r->stream), "subset back projection");
+        ESB_CK(launch_upsample(ks[j], r->slab_imgs, img, 1, W, H, os, 0, up, up_stride, r->stream),
+               "subset back projection");
+      }
+      ups[j - ch.first] = up;
+      off += cnt[j];
+    }
+    PhaseScope ps(r, 1);
+    const int f = ch.first;
+    const BpShape shape =
+        rec_bp_shape(r, ks[f], voxel_type, r->slab_imgs, img, T[f], cf.ctf_mode ? 1 : 0, ups[0], up_stride);
+    ESB_CK(launch_bp_axis_set(&ks[f], ups, &T[f], ch.second, up_stride, vol, voxel_type, W, H, lambda, os, &shape,
+                              r->stream),
+           "subset back projection");
+  }
+  return ESB_OK;
+}
+
 extern "C" {
 
 int esb_rec_back_projection(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, int voxel_type, int index,
@@ -1323,7 +1430,13 @@ static int sart_iteration(esb_reconstructor* r, const esb_vol_geom* vg, void* vo
       ESB_CK(cudaMemcpyAsync(r->sirt_d[i], r->proj_d, img * sizeof(float), cudaMemcpyDeviceToDevice, r->stream),
              "esb_sart_run");
     }
-    for (int i = 0; i < sirt_count; ++i) {
+    const int in_subset = std::min(sirt_count, proj_count - s * sirt_count);
+    bool fused = false;
+    if ((rc = rec_back_project_subset(r, vg, vol, voxel_type, index_list + s * sirt_count, in_subset,
+                                      (float)sirt_count, r->sirt_d.data(), fused)))
+      return rc;
+    if (fused) *volume_is_empty = 0;
+    for (int i = 0; i < sirt_count && !fused; ++i) {
       if (s * sirt_count + i >= proj_count) continue;
       *volume_is_empty = 0;
       const int index = index_list[s * sirt_count + i];
@@ -1651,7 +1764,13 @@ int esb_sart_run_zslab(esb_reconstructor* r, const esb_vol_geom* vg, void* vol, 
         ESB_CK(cudaMemcpyAsync(r->sirt_d[i], r->proj_d, img * sizeof(float), cudaMemcpyDeviceToDevice, r->stream),
                where);
       }
-      for (int i = 0; i < sirt_count; ++i) {
+      const int in_subset = std::min(sirt_count, proj_count - s * sirt_count);
+      bool fused = false;
+      if ((rc = rec_back_project_subset(r, vg, vol, voxel_type, index_list + s * sirt_count, in_subset,
+                                        (float)sirt_count, r->sirt_d.data(), fused)))
+        return rc;
+      if (fused) *volume_is_empty = 0;
+      for (int i = 0; i < sirt_count && !fused; ++i) {
         if (s * sirt_count + i >= proj_count) continue;
         *volume_is_empty = 0;
         const int index = index_list[s * sirt_count + i];
@@ -1704,6 +1823,35 @@ int esb_subvolume_wbp(esb_reconstructor* r, const esb_vol_geom* full_vol, int n_
                  "esb_subvolume_wbp");
         }
         return ok();
+      }
+      if (r->subvol_patches) {
+        // every tilt's slab images filtered and the patches its pairs read
+        // gathered (up to 16 GiB), then all tilts in one persistent launch
+        std::vector<SlabTable> Ts(proj_count);
+        for (int ii = 0; ii < proj_count; ++ii)
+          if ((rc = rec_slab_table(r, full_vol, index_list[ii], Ts[ii]))) return rc;
+        bool planned = false;
+        ESB_CK(subvol_patch_plan(r->batch, Ts.data(), W, H, (size_t)16 << 30, r->stream, planned),
+               "esb_subvolume_wbp");
+        if (planned) {
+          for (int ii = 0; ii < proj_count; ++ii) {
+            const int index = index_list[ii];
+            SlabTable T;
+            if ((rc = rec_subvol_slab_images(r, full_vol, projections + (size_t)index * img, index, T))) return rc;
+            PhaseScope ps(r, 3);
+            ESB_CK(subvol_patch_gather(r->batch, ii, r->slab_imgs, img, W, H, r->stream), "esb_subvolume_wbp");
+          }
+          {
+            PhaseScope ps(r, 1);
+            ESB_CK(subvol_patch_launch(r->batch, W, H, cf.oversampling, 1, r->stream), "esb_subvolume_wbp");
+          }
+          unsigned long long misses = 0;
+          ESB_CK(subvol_patch_misses(r->batch, r->stream, misses), "esb_subvolume_wbp");
+          if (misses)
+            return fail(ESB_ERR_UNSUPPORTED, "esb_subvolume_wbp: " + std::to_string(misses) +
+                                                 " quad samples fell outside the planned CTF patches");
+          return ok();
+        }
       }
       for (int ii = 0; ii < proj_count; ++ii) {
         const int index = index_list[ii];

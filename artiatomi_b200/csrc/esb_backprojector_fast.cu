@@ -169,6 +169,96 @@ __global__ void __launch_bounds__(128) k_bp_axis(KConst k, AxisGeom g, void* __r
   }
 }
 
+// One ordered subset back-projected in one pass over the volume (the
+// SIRTCount back-projections of EmSart.cpp:649-673): each quad is read once,
+// the updates of the subset's projections are added to it in the order of
+// the subset, as the per-projection launches add them, and it is stored once.
+// Every projection contributes exactly what k_bp_axis<VT, true> adds for it
+// (pre-sampled slab images, CTF slab chosen by the first corner's depth).
+// FP32 volumes: the result is bit for bit that of the per-projection
+// launches. FP16 / BF16 volumes: the sum is rounded to the storage type once
+// per subset instead of once per projection.
+struct BpSetItem {
+  KConst k;
+  AxisGeom a;
+  const float2* up;  // pre-sampled slab images of this projection
+  int nslab;         // 0: no CTF slabs
+  float bound[ESB_BP_SET_MAX_SLABS + 1];
+};
+struct BpSet {
+  int count;
+  size_t up_stride;
+  BpSetItem p[ESB_BP_SET_MAX];
+};
+
+template <int VT>
+__global__ void __launch_bounds__(128) k_bp_axis_set(const __grid_constant__ BpSet set, void* __restrict__ vol,
+                                                     int pw, int ph, float lambda, int os, float inv) {
+  const int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int z = (int)blockIdx.z;
+  const KConst& k0 = set.p[0].k;
+  const int ny = (int)k0.dim.y, nz = (int)k0.dim.z;
+  if (q >= k0.dimXQuarter || y >= ny || z >= nz) return;
+  const int x = 4 * q;
+  const long base = ((long)z * ny + y) * (long)k0.dim.x + x;
+  const bool vec = VT == ESB_VOXEL_F32 && (((uintptr_t)((float*)vol + base)) & 15) == 0;
+  float v[4];
+  if (vec) {
+    const float4 t = *((const float4*)((const float*)vol + base));
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = Voxel<VT>::loadrw(vol, base + i);
+  }
+  const int upH = ph * os;
+  const float fos = (float)os;
+  bool touched = false;
+#pragma unroll 1
+  for (int j = 0; j < set.count; ++j) {
+    const BpSetItem& it = set.p[j];
+    const KConst& k = it.k;
+    const AxisGeom& g = it.a;
+    const float depth = macro_depth(k, x, y, z);
+    const float2* up = it.up;
+    if (it.nslab > 0) {
+      if (!(depth >= it.bound[0] && depth < it.bound[it.nslab])) continue;
+      int s = 0;
+      while (s + 1 < it.nslab && depth >= it.bound[s + 1]) ++s;
+      up += (size_t)s * set.up_stride;
+    }
+    int pbx, pby, pbz, pbw;
+    if (g.clips) {
+      float d;
+      macro_footprint(k, x, y, z, pw, ph, d, pbx, pby, pbz, pbw);
+    } else {
+      macro_rect(g, x, y, z, pw, ph, pbx, pby, pbz, pbw);
+    }
+    const float cy = k.bbMin.y + ((float)y + 0.5f) * k.vs.y, cz = k.bbMin.z + ((float)z + 0.5f) * k.vs.z;
+    const float uyz = g.U.y * cy + g.U.z * cz + g.U0, vyz = g.V.y * cy + g.V.z * cz + g.V0;
+    const float dwv = inv * g.wv;
+    auto read = [&](int mu, int mv) -> float2 { return __ldg(up + (size_t)mu * upH + mv); };
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float cx = k.bbMin.x + ((float)(x + i) + 0.5f) * k.vs.x;
+      const float uc = g.U.x * cx + uyz, vc = g.V.x * cx + vyz;
+      float res, has;
+      axis_sums_rows(g, uc, vc, fos, inv, dwv, y, pbx * os, pby * os - 1, pbz * os, pbw * os - 1, read, res, has);
+      if (has > 0.f) {
+        v[i] += __fdividef(lambda * res, has);
+        touched = true;
+      }
+    }
+  }
+  if (!touched) return;
+  if (vec) {
+    *((float4*)((float*)vol + base)) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) Voxel<VT>::store(vol, base + i, v[i]);
+  }
+}
+
 // The slab images (transposed, [x][y], stride img_stride) sampled at every
 // sub-pixel grid point, with the voxel row of the grid point's ray:
 // up[s][mu][mv] = (image s at ((mu + 0.5) / os, (mv + 0.5) / os), row as int
@@ -238,6 +328,53 @@ cudaError_t launch_bp_fast(const KConst& k, void* vol, int vt, const float* img,
   none.count = 0;
   return launch_bp_fast_slabs(k, vol, vt, img, 0, none, pw, ph, pitchE, lambda, os, distMin, distMax, linear, st, 0,
                               nullptr, 0, nullptr);
+}
+
+// Whether projection k can join a subset launch (launch_bp_axis_set): the
+// single-axis kernel on pre-sampled images, at most ESB_BP_SET_MAX_SLABS
+// CTF slabs.
+bool bp_set_eligible(const KConst& k, int os, int nslab) {
+  const BpGeom g = make_geom(k, os);
+  return axis_eligible(k, g) && g.exact_grid && g.aniso_identity && nslab <= ESB_BP_SET_MAX_SLABS;
+}
+
+// The back-projections of `count` (<= ESB_BP_SET_MAX) projections of one
+// ordered subset in one launch (k_bp_axis_set): ks[j] the constants of
+// projection j, ups[j] its pre-sampled slab images (up_stride apart),
+// slabs[j] its CTF slabs (count 0: none); all bp_set_eligible, all on the
+// same volume geometry. The block shape is shape's (bx, by); its planes are
+// the whole volume.
+cudaError_t launch_bp_axis_set(const KConst* ks, const float2* const* ups, const SlabTable* slabs, int count,
+                               size_t up_stride, void* vol, int vt, int pw, int ph, float lambda, int os,
+                               const BpShape* shape, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  if (count > ESB_BP_SET_MAX) return cudaErrorInvalidValue;
+  const KConst& k0 = ks[0];
+  const int nq = k0.dimXQuarter, ny = (int)k0.dim.y, nz = (int)k0.dim.z;
+  if (nq <= 0 || ny <= 0 || nz <= 0) return cudaSuccess;
+  BpSet set;  // the kernel parameter (copied into the launch)
+  set.count = count;
+  set.up_stride = up_stride;
+  for (int j = 0; j < count; ++j) {
+    const BpGeom g = make_geom(ks[j], os);
+    if (!(axis_eligible(ks[j], g) && g.exact_grid && g.aniso_identity) || slabs[j].count > ESB_BP_SET_MAX_SLABS ||
+        !ups[j])
+      return cudaErrorInvalidValue;
+    BpSetItem& it = set.p[j];
+    it.k = ks[j];
+    it.a = make_axis_geom(ks[j], g, os);
+    it.up = ups[j];
+    it.nslab = slabs[j].count;
+    for (int b = 0; b <= it.nslab; ++b) it.bound[b] = slabs[j].bound[b];
+  }
+  const int bx = shape ? shape->bx : 32, by = shape ? shape->by : 4;
+  const dim3 blk(bx, by, 1), grd((nq + bx - 1) / bx, (ny + by - 1) / by, nz);
+  const float inv = 1.0f / (float)os;
+  if (vt == ESB_VOXEL_F32) k_bp_axis_set<ESB_VOXEL_F32><<<grd, blk, 0, st>>>(set, vol, pw, ph, lambda, os, inv);
+  else if (vt == ESB_VOXEL_F16) k_bp_axis_set<ESB_VOXEL_F16><<<grd, blk, 0, st>>>(set, vol, pw, ph, lambda, os, inv);
+  else k_bp_axis_set<ESB_VOXEL_BF16><<<grd, blk, 0, st>>>(set, vol, pw, ph, lambda, os, inv);
+  ESB_COUNT_LAUNCH();
+  return cudaGetLastError();
 }
 
 // Pre-sampled slab images for k_bp_fast / k_bp_axis (transposed input

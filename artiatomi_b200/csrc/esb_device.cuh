@@ -55,6 +55,11 @@ struct SlabTable {
   float bound[ESB_MAX_SLABS + 1];
 };
 
+// The subset back-projection (launch_bp_axis_set): up to ESB_BP_SET_MAX
+// projections in one launch, each with up to ESB_BP_SET_MAX_SLABS CTF slabs.
+#define ESB_BP_SET_MAX 8
+#define ESB_BP_SET_MAX_SLABS 64
+
 // Constants of kernel `ctf` (SetConstantValues(CTFKernel...), Kernels.cpp:1104-1131).
 struct CtfConst {
   float cs, lambda, ampC, phaseC, freqStep, pixelcount;

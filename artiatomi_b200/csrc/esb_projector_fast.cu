@@ -417,6 +417,29 @@ __device__ __forceinline__ float ldv(const char* p) {
   return __bfloat162float(__ldg((const __nv_bfloat16*)p));
 }
 
+// A voxel as loaded (float, or the 16 bits of a half / bfloat16), converted
+// to float where it is used: the walk's prefetched far row stays in its
+// loaded form until the next layer blends it.
+template <int VT>
+struct RawVoxel {
+  typedef unsigned short T;
+};
+template <>
+struct RawVoxel<ESB_VOXEL_F32> {
+  typedef float T;
+};
+template <int VT>
+__device__ __forceinline__ typename RawVoxel<VT>::T ldraw(const char* p) {
+  if constexpr (VT == ESB_VOXEL_F32) return __ldg((const float*)p);
+  else return __ldg((const unsigned short*)p);
+}
+template <int VT>
+__device__ __forceinline__ float cvt(typename RawVoxel<VT>::T r) {
+  if constexpr (VT == ESB_VOXEL_F32) return r;
+  else if constexpr (VT == ESB_VOXEL_F16) return __half2float(__ushort_as_half(r));
+  else return __uint_as_float((unsigned)r << 16);
+}
+
 // Sum of the trilinear interpolant over samples j0 .. J-1 of one ray whose y
 // interpolation coordinate lies in cell iy with weight b, walked along major
 // axis z (ZMAJ) or x with step signs SM (major) and SN (minor). Mq, Nq,
@@ -458,18 +481,18 @@ __device__ float axis_walk(const Cell<VT>& C, float Mq, float Nq, float dM, floa
   // raw far-row values (plane iy, plane iy + 1 at minor positions 0..3)
   // of the layer whose far row is at major index mi and window start ni
   const bool canN = nN >= 4;
-  float r0, r1, r2, r3, r4, r5, r6, r7;
+  typename RawVoxel<VT>::T r0, r1, r2, r3, r4, r5, r6, r7;
   auto fetch = [&](int mi, int ni, const char* q) {
     const int lo = SN > 0 ? ni : ni - 3;
     if (canN && (unsigned)lo <= (unsigned)(nN - 4) && (unsigned)mi < (unsigned)nM) {
-      r0 = ldv<VT>(q);
-      r1 = ldv<VT>(q + dy);
-      r2 = ldv<VT>(q + strideN);
-      r3 = ldv<VT>(q + strideN + dy);
-      r4 = ldv<VT>(q + 2 * strideN);
-      r5 = ldv<VT>(q + 2 * strideN + dy);
-      r6 = ldv<VT>(q + 3 * strideN);
-      r7 = ldv<VT>(q + 3 * strideN + dy);
+      r0 = ldraw<VT>(q);
+      r1 = ldraw<VT>(q + dy);
+      r2 = ldraw<VT>(q + strideN);
+      r3 = ldraw<VT>(q + strideN + dy);
+      r4 = ldraw<VT>(q + 2 * strideN);
+      r5 = ldraw<VT>(q + 2 * strideN + dy);
+      r6 = ldraw<VT>(q + 3 * strideN);
+      r7 = ldraw<VT>(q + 3 * strideN + dy);
     } else {
       mi = mi < 0 ? 0 : (mi > nM - 1 ? nM - 1 : mi);
       const char* row = base + ES * ((long)mi * sM + y0);
@@ -481,20 +504,20 @@ __device__ float axis_walk(const Cell<VT>& C, float Mq, float Nq, float dM, floa
       const char* q1 = at(ni + SN);
       const char* q2 = at(ni + 2 * SN);
       const char* q3 = at(ni + 3 * SN);
-      r0 = ldv<VT>(q0);
-      r1 = ldv<VT>(q0 + dy);
-      r2 = ldv<VT>(q1);
-      r3 = ldv<VT>(q1 + dy);
-      r4 = ldv<VT>(q2);
-      r5 = ldv<VT>(q2 + dy);
-      r6 = ldv<VT>(q3);
-      r7 = ldv<VT>(q3 + dy);
+      r0 = ldraw<VT>(q0);
+      r1 = ldraw<VT>(q0 + dy);
+      r2 = ldraw<VT>(q1);
+      r3 = ldraw<VT>(q1 + dy);
+      r4 = ldraw<VT>(q2);
+      r5 = ldraw<VT>(q2 + dy);
+      r6 = ldraw<VT>(q3);
+      r7 = ldraw<VT>(q3 + dy);
     }
   };
   // near row of the first layer, and its far row
   float N0 = ld(im - SM, in0), N1 = ld(im - SM, in0 + SN), N2 = ld(im - SM, in0 + 2 * SN);
   fetch(im, in0, P);
-  float F0 = fmaf(b, r1, ib * r0), F1 = fmaf(b, r3, ib * r2), F2 = fmaf(b, r5, ib * r4), F3 = fmaf(b, r7, ib * r6);
+  float F0 = fmaf(b, cvt<VT>(r1), ib * cvt<VT>(r0)), F1 = fmaf(b, cvt<VT>(r3), ib * cvt<VT>(r2)), F2 = fmaf(b, cvt<VT>(r5), ib * cvt<VT>(r4)), F3 = fmaf(b, cvt<VT>(r7), ib * cvt<VT>(r6));
   float fm0 = 0.0f, acc = 0.0f;
 #pragma unroll 1
   for (int guard = 0; guard < 1 << 20; ++guard) {
@@ -529,10 +552,10 @@ __device__ float axis_walk(const Cell<VT>& C, float Mq, float Nq, float dM, floa
     N0 = X ? F1 : F0;
     N1 = X ? F2 : F1;
     N2 = X ? F3 : F2;
-    F0 = fmaf(b, r1, ib * r0);
-    F1 = fmaf(b, r3, ib * r2);
-    F2 = fmaf(b, r5, ib * r4);
-    F3 = fmaf(b, r7, ib * r6);
+    F0 = fmaf(b, cvt<VT>(r1), ib * cvt<VT>(r0));
+    F1 = fmaf(b, cvt<VT>(r3), ib * cvt<VT>(r2));
+    F2 = fmaf(b, cvt<VT>(r5), ib * cvt<VT>(r4));
+    F3 = fmaf(b, cvt<VT>(r7), ib * cvt<VT>(r6));
     if (X) {
       fcn += 1.f;
       nNs = ((fcn + 1.f) - pN) * isN;
@@ -616,8 +639,10 @@ __global__ void __launch_bounds__(256) k_project_axis(KConst c, const void* __re
 }
 
 // k_slicer_fused for single-axis series; layout of k_slicer_fused.
+// (80 registers, 3 blocks per SM: uncapped, the 16-bit volume instances
+// take about 100 and fit 2)
 template <int VT, bool ZMAJ, int SM, int SN>
-__global__ void __launch_bounds__(256) k_slicer_axis(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
+__global__ void __launch_bounds__(256, 3) k_slicer_axis(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
                                                      size_t img_stride, size_t pitchE, SlabTable slabs, int x0, int y0,
                                                      int x1, int y1) {
   const int lane = threadIdx.x & 31;

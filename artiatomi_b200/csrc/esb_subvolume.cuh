@@ -44,7 +44,16 @@ struct SubvolBatch {
   size_t off_parts = 0, off_pairs = 0;
   int n_work = 0;
   int n_list = 0;
+  int n_particles = 0;
   int all_axis = 0;  // every pair takes the single-axis sums
+  // CTF patches (subvol_patch_plan): per pair the part of its tilt's slab
+  // images that the box's quads read, gathered into one buffer
+  void* pdev = nullptr;  // patch table, slab tables, miss counter
+  size_t pcap = 0;
+  std::vector<unsigned char> phost;
+  size_t off_slabs = 0, off_miss = 0;
+  float* patches = nullptr;
+  size_t patches_cap = 0;  // floats
 };
 
 // True when every box can be updated with aligned float4 accesses (x extent a
@@ -62,6 +71,27 @@ cudaError_t subvol_batch_build(SubvolBatch& b, int n_particles, float* const* bo
 // ([x][y]).
 cudaError_t subvol_batch_launch(const SubvolBatch& b, int t0, int nt, const float* imgs, size_t img_stride,
                                 const SlabTable& slabs, int pw, int ph, int os, int linear, cudaStream_t st);
+
+// With CTF: plans, for every (particle, list position) pair, the patch of
+// the position's slab images (slabs[t], images transposed, pw x ph) that the
+// particle's quads read: the slabs its depth range meets, and the detector
+// rectangle of its box's shadow with a margin, out-of-image texels held as
+// their clamped values. ok is false (nothing planned) when some pair does
+// not take the single-axis sums or the patches exceed max_bytes.
+cudaError_t subvol_patch_plan(SubvolBatch& b, const SlabTable* slabs, int pw, int ph, size_t max_bytes,
+                              cudaStream_t st, bool& ok);
+
+// Copies list position t's patches out of its slab images.
+cudaError_t subvol_patch_gather(const SubvolBatch& b, int t, const float* imgs, size_t img_stride, int pw, int ph,
+                                cudaStream_t st);
+
+// Adds every list position to every box in one persistent launch, reading
+// the patches.
+cudaError_t subvol_patch_launch(const SubvolBatch& b, int pw, int ph, int os, int linear, cudaStream_t st);
+
+// Number of (quad, position) pairs whose samples the plan did not cover
+// (skipped, so nothing was read outside the patches); synchronises.
+cudaError_t subvol_patch_misses(const SubvolBatch& b, cudaStream_t st, unsigned long long& misses);
 
 void subvol_batch_free(SubvolBatch& b);
 

@@ -452,6 +452,18 @@ class Reconstructor:
         captured on iteration 2."""
         check(lib.esb_reconstructor_enable_graphs(self._h, int(on)))
 
+    def fuse_subsets(self, on=True):
+        """Back-project each ordered subset of sart() in one volume pass:
+        True, False, or None for the default (FP16 / BF16 volumes only).
+        FP32 volumes come out bit for bit as with one pass per projection."""
+        check(lib.esb_reconstructor_fuse_subsets(self._h, -1 if on is None else int(bool(on))))
+
+    def subvolume_patches(self, on: bool = True):
+        """subvolume_wbp with CTF: all tilts in one launch from gathered
+        slab-image patches, else (the default) one launch per tilt; the
+        same boxes bit for bit."""
+        check(lib.esb_reconstructor_subvolume_patches(self._h, int(on)))
+
     def timing(self):
         """{phase: (ms, launches)} since the previous call; phases fp, bp, ctf, compare."""
         ms = np.zeros(4, np.float64)

@@ -11,14 +11,17 @@ tomogram frame, cubic boxes of 48/64/96 voxels in a 50/35/15 split, 61 tilts
 projections are synthetic: random ellipses with the line-integral profile of
 an ellipsoid plus Gaussian noise, made on the GPU.
 
-Both paths run through esb_subvolume_wbp: batched = 1 (FAST variant) runs
-one persistent launch over all particles (per tilt with CTF, over all tilts
-without); batched = 0 launches the back-projection once per particle per
-tilt, with the FAST kernel (all slabs of a tilt in one launch, --plain fast)
-or, as the reference does, with the FAITHFUL kernel once per particle per
-slab (--plain faithful). Prints one JSON line with both timings
-(CUDA events around the whole call, and the back-projection phase alone),
-the speed-up and the relative L2 difference of the two results.
+All paths run through esb_subvolume_wbp: batched = 1 (FAST variant) runs
+one persistent launch over all particles and all tilts (with CTF from the
+slab-image patches gathered after each tilt's CTF chain); with CTF the
+per_tilt arm runs it once per tilt over the whole slab images
+(esb_reconstructor_subvolume_patches off); batched = 0 launches the
+back-projection once per particle per tilt, with the FAST kernel (all slabs
+of a tilt in one launch, --plain fast) or, as the reference does, with the
+FAITHFUL kernel once per particle per slab (--plain faithful). Prints one
+JSON line with the timings (CUDA events around the whole call, and the
+back-projection phase alone), the speed-ups and the relative L2 difference
+of the results.
 """
 from __future__ import annotations
 
@@ -109,58 +112,75 @@ def main(argv=None):
     w = build(a.particles, a.frame, W, H, a.n_proj, a.os, not a.no_ctf, a.seed)
     projs = synthetic_projections(a.n_proj, W, H, a.seed + 1)
     il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, w["tilt"])
-    rec = E.Reconstructor(w["cfg"], w["pg"], w["tilt"], w["defocus"])
     plain_cfg = dataclasses.replace(w["cfg"], variant=E.VARIANT_FAST if a.plain == "fast" else E.VARIANT_FAITHFUL)
-    rec_plain = E.Reconstructor(plain_cfg, w["pg"], w["tilt"], w["defocus"])
-    recs = {False: rec_plain, True: rec}
-    boxes = {b: [torch.zeros((int(s),) * 3, dtype=torch.float32, device="cuda") for s in w["sizes"]]
-             for b in (False, True)}
+    # arms: plain (one launch per particle per tilt), per_tilt (batched, one
+    # launch per tilt over all boxes), batched (with CTF: all tilts in one
+    # launch from the gathered slab-image patches)
+    arms = ("plain", "per_tilt", "batched") if not a.no_ctf else ("plain", "batched")
+    recs = {}
+    for arm in arms:
+        recs[arm] = E.Reconstructor(plain_cfg if arm == "plain" else w["cfg"], w["pg"], w["tilt"], w["defocus"])
+        recs[arm].subvolume_patches(arm == "batched")  # per_tilt: the library's default
+    boxes = {arm: [torch.zeros((int(s),) * 3, dtype=torch.float32, device="cuda") for s in w["sizes"]]
+             for arm in arms}
     torch.cuda.synchronize()
     t_build = time.time() - t_build
 
-    def run(batched):
-        for b in boxes[batched]:
+    def run(arm):
+        for b in boxes[arm]:
             b.zero_()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        recs[batched].subvolume_wbp(w["full"], w["sub"], w["pair"], boxes[batched], projs, il, batched=batched)
+        recs[arm].subvolume_wbp(w["full"], w["sub"], w["pair"], boxes[arm], projs, il, batched=arm != "plain")
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
     res = {}
-    for batched in (False, True):
+    for arm in arms:
         for _ in range(a.warmup):
-            run(batched)
-        ms = [run(batched) for _ in range(a.reps)]
+            run(arm)
+        ms = [run(arm) for _ in range(a.reps)]
         # phase breakdown from one more run with per-launch events (kept out
         # of the timed runs: they add host work per launch)
-        recs[batched].enable_timing(True)
-        recs[batched].timing()
-        run(batched)
-        ph = recs[batched].timing()
-        recs[batched].enable_timing(False)
-        res[batched] = dict(ms=float(np.median(ms)), bp_ms=ph["bp"][0], bp_launches=ph["bp"][1], ctf_ms=ph["ctf"][0])
-    num = sum(float(((x - y).double() ** 2).sum()) for x, y in zip(boxes[True], boxes[False]))
-    den = sum(float((y.double() ** 2).sum()) for y in boxes[False])
+        recs[arm].enable_timing(True)
+        recs[arm].timing()
+        run(arm)
+        ph = recs[arm].timing()
+        recs[arm].enable_timing(False)
+        res[arm] = dict(ms=float(np.median(ms)), bp_ms=ph["bp"][0], bp_launches=ph["bp"][1], ctf_ms=ph["ctf"][0],
+                        gather_ms=ph["compare"][0])
+
+    def rel(x_arm, y_arm):
+        num = sum(float(((x - y).double() ** 2).sum()) for x, y in zip(boxes[x_arm], boxes[y_arm]))
+        den = sum(float((y.double() ** 2).sum()) for y in boxes[y_arm])
+        return float(np.sqrt(num / max(den, 1e-300)))
+
     voxels = int(sum(int(s) ** 3 for s in w["sizes"]))
     updates = voxels * len(il)
-    rec.close()
-    rec_plain.close()
-    print(json.dumps({
+    for r in recs.values():
+        r.close()
+    out = {
         "workload": "subvolume_wbp", "particles": a.particles, "frame": a.frame, "proj": [W, H],
         "n_proj": a.n_proj, "oversampling": a.os, "ctf": not a.no_ctf, "voxels": voxels, "plain": a.plain,
-        "plain_ms": res[False]["ms"], "batched_ms": res[True]["ms"],
-        "speedup": res[False]["ms"] / res[True]["ms"],
-        "plain_bp_ms": res[False]["bp_ms"], "batched_bp_ms": res[True]["bp_ms"],
-        "bp_speedup": res[False]["bp_ms"] / max(res[True]["bp_ms"], 1e-9),
-        "plain_bp_launches": res[False]["bp_launches"], "batched_bp_launches": res[True]["bp_launches"],
-        "plain_ctf_ms": res[False]["ctf_ms"], "batched_ctf_ms": res[True]["ctf_ms"],
-        "batched_voxel_updates_per_s": updates / (res[True]["ms"] * 1e-3),
-        "rel_l2_batched_vs_plain": float(np.sqrt(num / max(den, 1e-300))),
+        "plain_ms": res["plain"]["ms"], "batched_ms": res["batched"]["ms"],
+        "speedup": res["plain"]["ms"] / res["batched"]["ms"],
+        "plain_bp_ms": res["plain"]["bp_ms"], "batched_bp_ms": res["batched"]["bp_ms"],
+        "bp_speedup": res["plain"]["bp_ms"] / max(res["batched"]["bp_ms"], 1e-9),
+        "plain_bp_launches": res["plain"]["bp_launches"], "batched_bp_launches": res["batched"]["bp_launches"],
+        "plain_ctf_ms": res["plain"]["ctf_ms"], "batched_ctf_ms": res["batched"]["ctf_ms"],
+        "batched_voxel_updates_per_s": updates / (res["batched"]["ms"] * 1e-3),
+        "rel_l2_batched_vs_plain": rel("batched", "plain"),
         "setup_s": round(t_build, 1),
-    }))
+    }
+    if "per_tilt" in res:
+        out.update({"per_tilt_ms": res["per_tilt"]["ms"], "per_tilt_bp_ms": res["per_tilt"]["bp_ms"],
+                    "per_tilt_bp_launches": res["per_tilt"]["bp_launches"],
+                    "batched_gather_ms": res["batched"]["gather_ms"],
+                    "speedup_vs_per_tilt": res["per_tilt"]["ms"] / res["batched"]["ms"],
+                    "batched_equals_per_tilt": rel("batched", "per_tilt") == 0.0})
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":

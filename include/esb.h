@@ -371,6 +371,28 @@ int esb_reconstructor_timing(esb_reconstructor* rec, double out_ms[4], int count
  * graph). */
 int esb_reconstructor_enable_graphs(esb_reconstructor* rec, int enable);
 
+/* Back-projects each ordered subset of esb_sart_run / esb_sart_run_zslab in
+ * one pass over the volume: every voxel is read once per subset, the
+ * SIRTCount updates are added to it in the subset's order, and it is stored
+ * once. FP32 volumes come out bit for bit as with one pass per projection
+ * (EmSart.cpp:649-673); FP16 / BF16 volumes are rounded once per subset
+ * instead of once per projection. enable: 1 on, 0 off, -1 (the default) on
+ * for FP16 / BF16 volumes only (for FP32 the one-pass launch is no faster:
+ * the back-projection is bound by instruction issue, not by volume traffic).
+ * Applies to the FAST variant on single-axis geometry without magnification
+ * anisotropy, power-of-two oversampling and at most 64 CTF slabs per
+ * projection; other subsets are back-projected one projection at a time. */
+int esb_reconstructor_fuse_subsets(esb_reconstructor* rec, int enable);
+
+/* esb_subvolume_wbp with CTF, batched: on, after each tilt's CTF chain the
+ * parts of its slab images that each particle's box reads are gathered into
+ * one patch buffer (up to 16 GiB), and one persistent launch adds every tilt
+ * to every box, each box read and written once. Off (the default): one
+ * launch per tilt over all boxes, which is as fast (the back-projection is
+ * bound by instruction issue, not by box traffic). Both give the same boxes
+ * bit for bit. */
+int esb_reconstructor_subvolume_patches(esb_reconstructor* rec, int enable);
+
 /* ResetProjectionsDevice (Reconstructor.cpp:1678-1682). */
 int esb_rec_reset_projections(esb_reconstructor* rec);
 /* ForwardProjection (Reconstructor.cpp:1411-1421), CTF or not. */

@@ -236,12 +236,14 @@ def _subvolume_case(ctf, sizes, n=7, seed=31, psi_deg=0.0):
                 pair_o=pair_o, defocus=defocus if ctf else None, cfgd=cfgd, shifts=shifts, sizes=sizes)
 
 
-def _subvolume_gpu(c, batched, index_list, active=None):
+def _subvolume_gpu(c, batched, index_list, active=None, patches=None):
     import artiatomi_b200 as E
 
     W, H, n = c["W"], c["H"], c["n"]
     pg = E.projection_geometry(E.Markers(c["tilt"], rotation_psi=c["psi"]), W, H)
     rec = E.Reconstructor(E.ReconConfig(W, H, n, variant=E.VARIANT_FAST, **c["cfgd"]), pg, c["tilt"], c["defocus"])
+    if patches is not None:
+        rec.subvolume_patches(patches)
     boxes = [cuda(np.zeros((s, s, s), np.float32)) for s in c["sizes"]]
     rec.subvolume_wbp(c["full"], c["sub"], c["pair"], boxes, cuda(c["projs"]), index_list, active=active,
                       batched=batched)
@@ -295,6 +297,24 @@ def test_batched_subvolume_matches_per_particle(ctf):
     tol = 1e-3 if ctf else 1e-4
     for b, o in zip(batch, _subvolume_oracle(c, il, active)):
         assert rel_l2(b, o) <= tol
+
+
+@pytest.mark.parametrize("psi_deg", [0.0, 0.7])
+def test_subvolume_ctf_patches_match_per_tilt(psi_deg):
+    """With CTF the batched call gathers, after each tilt's CTF chain, the
+    patch of the slab images each box reads, and adds all tilts in one
+    launch (esb_reconstructor_subvolume_patches). One launch per tilt over
+    the whole slab images gives the same boxes bit for bit: the same sums in
+    the same order, patch texels equal to the clamped image texels (boxes
+    here reach past the detector edge). 4 nm slabs: boxes span several."""
+    c = _subvolume_case(True, [16, 24, 32, 48, 16, 24], n=9, seed=5, psi_deg=psi_deg)
+    il = np.random.default_rng(1).permutation(c["n"]).astype(np.int32)
+    active = (np.linalg.norm(c["shifts"], axis=2) < 1.5).astype(np.uint8)
+    one = _subvolume_gpu(c, True, il, active, patches=True)
+    per_tilt = _subvolume_gpu(c, True, il, active, patches=False)
+    for a, b in zip(per_tilt, one):
+        assert np.abs(a).sum() > 0
+        np.testing.assert_array_equal(b, a)
 
 
 def test_batched_subvolume_ragged_box_runs_per_particle():
