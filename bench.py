@@ -248,6 +248,22 @@ def run_reference(args):
     return 0
 
 
+def _mean_slabs(E, wl, params) -> float:
+    """CTF slabs per projection of the workload, averaged over its
+    projections: the library's slab recurrence (ray += thickness from the
+    volume's entry depth while ray < its exit depth, in float)."""
+    step = np.float32(wl.cfg.ctf_slice_thickness_nm) / np.float32(wl.cfg.pixel_size_nm)
+    counts = []
+    for i in wl.index_list:
+        t_in, t_out = E.defocus_distances(wl.pg[int(i)], wl.vg, params["W"], params["H"])
+        ray, k = np.float32(t_in), 0
+        while ray < np.float32(t_out):
+            ray = np.float32(ray + step)
+            k += 1
+        counts.append(k)
+    return float(np.mean(counts))
+
+
 def config_parity(name: str = "c2_crop") -> dict:
     """The SART volume of workload `name` (FAST kernels, this library)
     against the FP32 and FP64 CPU oracles, on the same measured projections."""
@@ -372,8 +388,10 @@ def run_esb(args):
         traffic = (DRAM_BP_READ + DRAM_BP_WRITE) / DRAM_V * V + DRAM_BP_IMG / DRAM_P * P
         name, t_unit, launches = "back-projection (all slab launches of one projection)", bp_ms / nproj, bp_n
     else:
-        slabs = (fp_n / nproj) - 1
-        bytes_unit = V * 4 + (2 * slabs + 2) * P * 4
+        slabs = _mean_slabs(E, wl, params) if params["ctf"] else 1.0
+        # the volume read once; per CTF slab one image written; the ray
+        # lengths written once
+        bytes_unit = V * 4 + (slabs + 1) * P * 4
         traffic = DRAM_FP_READ / DRAM_V * V + DRAM_FP_IMG / DRAM_P * P
         name, t_unit, launches = "forward projection (slicer launches + traversal length of one projection)", \
             fp_ms / nproj, fp_n

@@ -5,7 +5,7 @@ reference tree, and libesb for the device work), linked against
 artiatomi_b200/libesb.so and the CUDA runtime.
 
 TEST INFRASTRUCTURE: tests/test_cpp_caller.py runs it. Needs the reference
-tree (REF_ROOT, default /root/reference) and a built libesb.so; without the
+tree (oracle/refroot.py) and a built libesb.so; without the
 reference tree the build is skipped.
 """
 from __future__ import annotations

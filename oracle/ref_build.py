@@ -9,8 +9,7 @@ of the reference's .cu files from its place in the reference tree
 host against the CUDA-execution shim in oracle/ref_shim/ (esb_ref_shim.h and
 the stand-in headers in oracle/ref_shim/include/). The shared library goes to
 oracle/_ref/, which git ignores. It is used only to pin the oracle against
-the reference's own kernel code. Needs the reference tree (REF_ROOT, default
-/root/reference); without it the build is skipped.
+the reference's own kernel code. Needs the reference tree (oracle/refroot.py); without it the build is skipped.
 """
 from __future__ import annotations
 
@@ -23,7 +22,9 @@ HERE = Path(__file__).resolve().parent
 SHIM = HERE / "ref_shim"
 OUT = HERE / "_ref" / "libref_kernels.so"
 OUT_CTF_GPU = HERE / "_ref" / "libref_ctf_gpu.so"
-REF_ROOT = Path(os.environ.get("REF_ROOT", "/root/reference"))
+if str(HERE.parent) not in sys.path:
+    sys.path.insert(0, str(HERE.parent))
+from oracle.refroot import REF_ROOT  # noqa: E402
 KERNELS = REF_ROOT / "src" / "EmSART" / "cuda_kernels"
 UNITS = ["ref_runtime.cpp", "ref_fp.cpp", "ref_slicer.cpp", "ref_compare.cpp", "ref_bp.cpp", "ref_square.cpp",
          "ref_ctf.cpp", "ref_wbp.cpp"]

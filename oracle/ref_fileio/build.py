@@ -5,8 +5,7 @@ copied) linked with the harness oracle/ref_fileio/ref_fileio.cpp.
 
 TEST INFRASTRUCTURE: used by tests/test_fileio.py and
 tests/golden/make_fileio_golden.py to pin artiatomi_b200.fileio to the
-reference's readers and writers. Needs the reference tree (REF_ROOT,
-default /root/reference); without it the build is skipped.
+reference's readers and writers. Needs the reference tree (oracle/refroot.py); without it the build is skipped.
 """
 from __future__ import annotations
 
@@ -17,7 +16,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE.parent / "_ref" / "ref_fileio"
-REF_ROOT = Path(os.environ.get("REF_ROOT", "/root/reference"))
+if str(HERE.parent.parent) not in sys.path:
+    sys.path.insert(0, str(HERE.parent.parent))
+from oracle.refroot import REF_ROOT  # noqa: E402
 TOOLS = REF_ROOT / "src" / "EmTools"
 SOURCES = ["FileIO/EmFile.cpp", "FileIO/MRCFile.cpp", "FileIO/File.cpp", "FileIO/FileReader.cpp",
            "FileIO/FileWriter.cpp", "FileIO/FileIOException.cpp", "FileIO/ImageBase.cpp", "FileIO/MarkerFile.cpp",

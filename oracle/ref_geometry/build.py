@@ -6,8 +6,7 @@ linked with the harness oracle/ref_geometry/ref_geometry.cpp.
 
 TEST INFRASTRUCTURE: used by tests/golden/make_geometry_golden.py and
 tests/test_geometry_reference.py to pin the library's geometry to the
-reference's bit for bit. Needs the reference tree (REF_ROOT, default
-/root/reference); without it the build is skipped.
+reference's bit for bit. Needs the reference tree (oracle/refroot.py); without it the build is skipped.
 """
 from __future__ import annotations
 
@@ -18,7 +17,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE.parent / "_ref" / "ref_geometry"
-REF_ROOT = Path(os.environ.get("REF_ROOT", "/root/reference"))
+if str(HERE.parent.parent) not in sys.path:
+    sys.path.insert(0, str(HERE.parent.parent))
+from oracle.refroot import REF_ROOT  # noqa: E402
 SRC = REF_ROOT / "src"
 SOURCES = ["EmSART/Projection.cpp", "EmSART/Volume.cpp", "EmSART/utils/Config.cpp", "EmSART/utils/ConfigExceptions.cpp",
            "EmSART/utils/log.cpp", "EmTools/FileIO/MarkerFile.cpp", "EmTools/FileIO/ImodFiducialFile.cpp",

@@ -79,6 +79,42 @@ def test_integration_snippet_is_the_compiled_program():
     assert _norm(_snippet(SRC.read_text())) in _norm(doc)
 
 
+def _blocks(text: str, begin: str):
+    out, i = [], 0
+    while True:
+        a = text.find(begin, i)
+        if a < 0:
+            return out
+        a = text.index("\n", a) + 1
+        b = text.index("// --- end ---", a)
+        out.append(text[a:b])
+        i = b
+
+
+def test_zslab_nccl_caller_compiles_and_is_documented(tmp_path):
+    """The multi-GPU section's C++ (esb_sart_run_zslab with an NCCL
+    all-reduce callback) compiles against include/esb.h and nccl.h and
+    links against libesb and NCCL; INTEGRATION.md shows the same code."""
+    import shutil
+
+    src = ROOT / "oracle" / "cpp_caller" / "zslab_nccl.cpp"
+    text = src.read_text()
+    doc = _norm((ROOT / "INTEGRATION.md").read_text())
+    blocks = _blocks(text, "// --- begin: z-slab SART")
+    assert len(blocks) == 2
+    for b in blocks:
+        assert _norm(b) in doc
+    if not shutil.which("g++"):
+        pytest.skip("g++ not available")
+    cuda = Path("/usr/local/cuda/include")
+    r = subprocess.run(["g++", "-std=c++14", "-fPIC", "-shared", "-I", str(ROOT / "include"), "-I", str(cuda),
+                        str(src), "-L", str(ROOT / "artiatomi_b200"), "-lesb", "-lnccl",
+                        "-o", str(tmp_path / "libzslab.so")], capture_output=True, text=True)
+    if r.returncode != 0 and ("nccl.h" in r.stderr or "-lnccl" in r.stderr):
+        pytest.skip("NCCL headers or library not found: " + r.stderr.strip().splitlines()[-1])
+    assert r.returncode == 0, r.stderr
+
+
 @pytest.mark.gpu
 def test_cpp_caller_sart_matches_oracle(tmp_path):
     if not EXE.exists():
