@@ -264,18 +264,22 @@ __global__ void __launch_bounds__(128) k_bp_axis_set(const __grid_constant__ BpS
 // up[s][mu][mv] = (image s at ((mu + 0.5) / os, (mv + 0.5) / os), row as int
 // bits), clamp addressing, nearest or bilinear as the back-projection reads
 // it (sample_row; meaningful for single-axis projections, which read it).
-__global__ void __launch_bounds__(256) k_upsample(const float* __restrict__ imgs, size_t img_stride, int pw, int ph,
-                                                  int os, float inv, int linear, RowGeom rg, float2* __restrict__ up,
-                                                  size_t up_stride) {
+// The row depends on the grid point and the projection only: it is formed
+// once per grid point and stored with the point's value in every slab image.
+__global__ void __launch_bounds__(256) k_upsample(const float* __restrict__ imgs, size_t img_stride, int count, int pw,
+                                                  int ph, int os, float inv, int linear, RowGeom rg,
+                                                  float2* __restrict__ up, size_t up_stride) {
   const int mv = blockIdx.x * blockDim.x + threadIdx.x;
   const int mu = blockIdx.y;
-  const int s = blockIdx.z;
   const int upH = ph * os;
   if (mv >= upH) return;
   const float px = ((float)mu + 0.5f) * inv, py = ((float)mv + 0.5f) * inv;
-  up[(size_t)s * up_stride + (size_t)mu * upH + mv] =
-      make_float2(sample_image(imgs + (size_t)s * img_stride, pw, ph, (size_t)pw, px, py, linear != 0, true),
-                  __int_as_float(sample_row(rg, mu, mv)));
+  const float row = __int_as_float(sample_row(rg, mu, mv));
+  float2* out = up + (size_t)mu * upH + mv;
+#pragma unroll 1
+  for (int s = 0; s < count; ++s)
+    out[(size_t)s * up_stride] =
+        make_float2(sample_image(imgs + (size_t)s * img_stride, pw, ph, (size_t)pw, px, py, linear != 0, true), row);
 }
 
 }  // namespace
@@ -383,9 +387,9 @@ cudaError_t launch_bp_axis_set(const KConst* ks, const float2* const* ups, const
 cudaError_t launch_upsample(const KConst& k, const float* imgs, size_t img_stride, int count, int pw, int ph, int os,
                             int linear, float2* up, size_t up_stride, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
-  dim3 blk(256), grd((ph * os + 255) / 256, pw * os, count);
-  k_upsample<<<grd, blk, 0, st>>>(imgs, img_stride, pw, ph, os, 1.0f / (float)os, linear, make_row_geom(k, os), up,
-                                  up_stride);
+  dim3 blk(256), grd((ph * os + 255) / 256, pw * os, 1);
+  k_upsample<<<grd, blk, 0, st>>>(imgs, img_stride, count, pw, ph, os, 1.0f / (float)os, linear, make_row_geom(k, os),
+                                  up, up_stride);
   ESB_COUNT_LAUNCH();
   return cudaGetLastError();
 }

@@ -639,10 +639,11 @@ __global__ void __launch_bounds__(256) k_project_axis(KConst c, const void* __re
 }
 
 // k_slicer_fused for single-axis series; layout of k_slicer_fused.
-// (80 registers, 3 blocks per SM: uncapped, the 16-bit volume instances
-// take about 100 and fit 2)
+// (16-bit volumes: at most 80 registers, 3 blocks of 256 threads per SM;
+// uncapped, those instances take about 100 and fit 2. FP32 instances take
+// 76-79 uncapped, and a cap changes their allocation for the worse.)
 template <int VT, bool ZMAJ, int SM, int SN>
-__global__ void __launch_bounds__(256, 3) k_slicer_axis(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
+__global__ void __launch_bounds__(256, VT == ESB_VOXEL_F32 ? 0 : 3) k_slicer_axis(KConst c, const void* __restrict__ vol, float* __restrict__ imgs,
                                                      size_t img_stride, size_t pitchE, SlabTable slabs, int x0, int y0,
                                                      int x1, int y1) {
   const int lane = threadIdx.x & 31;

@@ -71,12 +71,12 @@ UNIT = "voxel-updates/s"
 
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum,
 # dram__bytes_write.sum) on the 1024x1024x64 volume / 1024^2 detector case,
-# per unit of the roofline: forward projection = k_slicer_fused (volume read,
-# slab images written) + k_travlen (image read), back-projection = k_bp_axis
-# (volume read and written, pre-sampled slab images read). The volume part
-# scales with the voxels, the image part with the pixels.
+# per unit of the roofline: forward projection = k_slicer_axis (volume read,
+# slab images written) + k_travlen (ray lengths written), back-projection =
+# k_bp_axis (volume read and written, pre-sampled slab images read). The
+# volume part scales with the voxels, the image part with the pixels.
 DRAM_V, DRAM_P = 1024 * 1024 * 64, 1024 * 1024
-DRAM_FP_READ, DRAM_FP_IMG = 268.62e6, 4.74e6 + 4.20e6
+DRAM_FP_READ, DRAM_FP_IMG = 268.44e6, 8.47e6 + 4.20e6
 DRAM_BP_READ, DRAM_BP_WRITE, DRAM_BP_IMG = 268.44e6, 211.57e6, 292.94e6 - 268.44e6
 
 
@@ -265,18 +265,20 @@ def _mean_slabs(E, wl, params) -> float:
 
 
 def config_parity(name: str = "c2_crop") -> dict:
-    """The SART volume of workload `name` (FAST kernels, this library)
-    against the FP32 and FP64 CPU oracles, on the same measured projections."""
+    """The SART volume of workload `name` (this library's FAST kernels, and
+    its FAITHFUL ones) against the FP32 and FP64 CPU oracles, on the same
+    measured projections."""
     from oracle.parity import rel_l2, run_config
 
     t0 = time.perf_counter()
-    run = run_config(name, variants=("fast",), precisions=(0, 1))
+    run = run_config(name, variants=("fast", "faithful"), precisions=(0, 1))
     p = run.params
     return {"workload": name, "volume": list(p["dims"]), "projections": p["n_proj"], "iterations": p["iterations"],
             "oversampling": p["os"], "sirt_count": p["sirt"], "ctf": p["ctf"],
             "rel_l2_vs_fp32_oracle": rel_l2(run.volumes["fast"], run.oracle[0]),
             "rel_l2_vs_fp64_oracle": rel_l2(run.volumes["fast"], run.oracle[1]),
             "fp32_oracle_vs_fp64_oracle": rel_l2(run.oracle[0], run.oracle[1]),
+            "faithful_rel_l2_vs_fp32_oracle": rel_l2(run.volumes["faithful"], run.oracle[0]),
             "seconds": round(time.perf_counter() - t0, 1)}
 
 

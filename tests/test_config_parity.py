@@ -11,7 +11,7 @@ projections:
 - the C2 geometry cropped to 256x256x64: 61 tilts of 256^2 (2 degree steps)
   with per-tilt shifts U(+-2 px) and psi jitter +-0.3 deg, 3-D CTF over
   30 nm defocus slabs, oversampling 2, 4 projections per ordered subset,
-  2 iterations.
+  2 iterations (FAST and FAITHFUL).
 
 Tolerances. The FAITHFUL kernels restate the reference's FP32 arithmetic
 operation by operation and stay within 1e-5 of the FP32 oracle. The FAST
@@ -51,7 +51,7 @@ def c1():
 
 @pytest.fixture(scope="module")
 def c2crop():
-    return run_config("c2_crop", variants=("fast",), precisions=(0, 1))
+    return run_config("c2_crop", variants=("fast", "faithful"), precisions=(0, 1))
 
 
 def test_c1_full_size_fast_vs_fp32_oracle(c1):
@@ -88,3 +88,12 @@ def test_c2_crop_fast_vs_fp64_oracle(c2crop):
     print(f"C2 crop FAST vs FP64 oracle rel-L2 {e:.3e}; "
           f"FP32 oracle vs FP64 {rel_l2(c2crop.oracle[0], c2crop.oracle[1]):.3e}")
     assert e <= FAST_FP64_TOL, e
+
+
+def test_c2_crop_faithful_vs_fp32_oracle(c2crop):
+    """The reference's FP32 arithmetic at the C2 geometry (CTF slabs,
+    oversampling 2, subsets of 4, shifts and psi jitter): the FAITHFUL
+    kernels reproduce the FP32 oracle."""
+    e = rel_l2(c2crop.volumes["faithful"], c2crop.oracle[0])
+    print(f"C2 crop FAITHFUL vs FP32 oracle rel-L2 {e:.3e}")
+    assert e <= FAITHFUL_TOL, e
