@@ -71,13 +71,25 @@ class OracleSlab:
         pass
 
 
-def _oracle_slab(case, part, count):
+def _ctf_setup(ctf):
+    """(reconstructor config, defocus table) of the case, with or without
+    3-D CTF (2.5 nm slabs: several per slab of the volume)."""
+    if not ctf:
+        return dict(CFG), None
+    from tests.test_parity_fast import _defocus
+    from tests.test_parity_recon import _ctf_cfg
+
+    return dict(_ctf_cfg(W), **CFG), _defocus(N_PROJ, 15)
+
+
+def _oracle_slab(case, part, count, ctf=False):
     from oracle import geometry as G
     from oracle.driver import OracleReconstructor
 
+    cfgd, defocus = _ctf_setup(ctf)
     vo = G.volume_geometry(DIMS, count=count, part=part)
     vol = np.zeros((int(vo.dim[2]), DIMS[1], DIMS[0]), np.float32)
-    orc = OracleReconstructor(CFG, W, H, case["og"], case["tilt"])
+    orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], defocus)
     return OracleSlab(orc, vo, vol)
 
 
@@ -322,7 +334,7 @@ def test_reconstruct_subvolumes_particle_sharding_two_ranks():
     assert sorted(seen) == list(range(SUB_N))
 
 
-def _worker_gpu(rank, world, port, outdir):
+def _worker_gpu(rank, world, port, outdir, ctf):
     import torch
     import torch.distributed as dist
 
@@ -338,7 +350,9 @@ def _worker_gpu(rank, world, port, outdir):
         il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, case["tilt"])
         vg = E.volume_geometry(DIMS, subvol_count=world, subvol=rank)
         vol = torch.zeros((int(vg.dim[2]), DIMS[1], DIMS[0]), device="cuda")
-        rec = E.Reconstructor(E.ReconConfig(W, H, N_PROJ, variant=E.VARIANT_FAST, **CFG), case["pg"], case["tilt"])
+        cfgd, defocus = _ctf_setup(ctf)
+        rec = E.Reconstructor(E.ReconConfig(W, H, N_PROJ, variant=E.VARIANT_FAST, **cfgd), case["pg"], case["tilt"],
+                              defocus)
         empty = rec.sart_zslab(vg, vol, projs, il, 2, 2, torch_allreduce())
         assert not empty
         torch.cuda.synchronize()
@@ -349,7 +363,11 @@ def _worker_gpu(rank, world, port, outdir):
 
 
 @pytest.mark.gpu
-def test_zslab_sart_two_ranks_on_gpu():
+@pytest.mark.parametrize("ctf", [False, True])
+def test_zslab_sart_two_ranks_on_gpu(ctf):
+    """esb_sart_run_zslab in two processes (one slab each, the all-reduce
+    over gloo) equals the decomposition run in one process; with CTF each
+    rank filters its own slab images before the sum."""
     import torch
     import torch.multiprocessing as mp
 
@@ -357,7 +375,7 @@ def test_zslab_sart_two_ranks_on_gpu():
     from artiatomi_b200.distributed import GpuSlab
 
     with tempfile.TemporaryDirectory() as d:
-        mp.spawn(_worker_gpu, args=(2, _free_port(), d), nprocs=2, join=True)
+        mp.spawn(_worker_gpu, args=(2, _free_port(), d, ctf), nprocs=2, join=True)
         got = [np.load(os.path.join(d, f"slab{r}.npy")) for r in range(2)]
     case = _case()
     projs = torch.from_numpy(_projections(case)).cuda()
@@ -366,14 +384,16 @@ def test_zslab_sart_two_ranks_on_gpu():
     for r in range(2):
         vg = E.volume_geometry(DIMS, subvol_count=2, subvol=r)
         vol = torch.zeros((int(vg.dim[2]), DIMS[1], DIMS[0]), device="cuda")
-        rec = E.Reconstructor(E.ReconConfig(W, H, N_PROJ, variant=E.VARIANT_FAST, **CFG), case["pg"], case["tilt"])
+        cfgd, defocus = _ctf_setup(ctf)
+        rec = E.Reconstructor(E.ReconConfig(W, H, N_PROJ, variant=E.VARIANT_FAST, **cfgd), case["pg"], case["tilt"],
+                              defocus)
         slabs.append(GpuSlab(rec, vg, vol))
     _emulate(slabs, projs, il, 2, 2)
     torch.cuda.synchronize()
     for r in range(2):
         np.testing.assert_array_equal(got[r], slabs[r].vol.cpu().numpy())
     # and the oracle's decomposition, at the fast-kernel SART tolerance
-    oslabs = [_oracle_slab(case, r, 2) for r in range(2)]
+    oslabs = [_oracle_slab(case, r, 2, ctf) for r in range(2)]
     _emulate(oslabs, projs.cpu().numpy(), il, 2, 2)
     for r in range(2):
         assert rel_l2(got[r], oslabs[r].vol) <= 1e-3
