@@ -1,8 +1,8 @@
 """CPU oracle of the EmSART reconstruction hot path (TEST INFRASTRUCTURE).
 
 Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` import this package, and only as the checker or as the timed CPU
-baseline. The product (``artiatomi_b200``) never imports it.
+``bench.py`` import this package, and only as the reference the results are
+compared with or as the timed CPU baseline. The product (``artiatomi_b200``) never imports it.
 
 Layout:
   esb_oracle.cpp  - C++ restatement of the reference's device kernels

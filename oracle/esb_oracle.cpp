@@ -2,8 +2,8 @@
 //
 // TEST INFRASTRUCTURE ONLY. Nothing in the product library links, loads or
 // calls this file; only the tests, the smoke check and the CPU-baseline leg
-// of the benchmark do, and there only as the checker (or as the timed CPU
-// baseline).  It restates, statement by statement, the device code and the
+// of the benchmark do, and there only as what results are compared with (or
+// as the timed CPU baseline).  It restates, statement by statement, the device code and the
 // host geometry of uermel/Artiatomi's EmSART so that the CUDA kernels of this
 // repository can be compared against the reference's algorithm on the same
 // inputs.  Every function cites the reference file and lines it follows

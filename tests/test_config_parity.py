@@ -18,7 +18,7 @@ operation by operation and stay within 1e-5 of the FP32 oracle. The FAST
 kernels compute the reference's sums with exact chords and closed-form cell
 sums, i.e. the reference's algorithm without its float rounding: they are
 held to 2e-4 of the FP64 oracle (the reference's algorithm evaluated in
-double precision). Against the FP32 oracle the north-star bar is 1e-3, but
+double precision). Against the FP32 oracle the parity bar is 1e-3, but
 the reference's own FP32 rounding moves it from the FP64 result by about as
 much (its back-projection chords come from ray origins 1e5 units away,
 float noise ~1 % per chord: 1.13e-3 at C1 after 3 iterations). So the FAST
@@ -39,7 +39,7 @@ FAITHFUL_FP64_TOL = 2e-3
 
 
 def _fast_vs_fp32_bound(run):
-    """The north-star bar, or the reference's own FP32-vs-FP64 distance
+    """The parity bar, or the reference's own FP32-vs-FP64 distance
     (plus 1e-4) where that is larger."""
     return max(FAST_TOL, rel_l2(run.oracle[0], run.oracle[1]) + 1e-4)
 

@@ -9,7 +9,7 @@ chords carry rounding noise from ray origins 1e5 units away. On random
 images a single update differs from the exact (FP64) update by 0.3-1%
 rel-L2, and the FP32 oracle reproduces that noise. The fast kernel is held to
 the FP64 oracle per update (rel-L2 <= 1e-5) and to both oracles on SART
-volumes, the north-star measure (FP32: <= 1e-3; FP64: <= 2e-4).
+volumes, the parity measure (FP32: <= 1e-3; FP64: <= 2e-4).
 """
 import numpy as np
 import pytest

@@ -4,7 +4,7 @@ oracle's restatement of the reference kernel on the same seeded inputs.
 Tolerances. The faithful projector/back-projector evaluate the reference's
 float expressions in the same order as the FP32 oracle, so they agree to the
 last bits apart from summation order: rel-L2 <= 1e-5. Against the FP64 oracle
-the bar is the north-star 1e-3. The Fourier-space and image kernels use
+the bar is the parity bar of 1e-3. The Fourier-space and image kernels use
 CUDA's libm (expf, sinf, atan2f) against glibc/double: rel-L2 <= 1e-5.
 """
 import numpy as np
