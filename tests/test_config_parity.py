@@ -97,3 +97,17 @@ def test_c2_crop_faithful_vs_fp32_oracle(c2crop):
     e = rel_l2(c2crop.volumes["faithful"], c2crop.oracle[0])
     print(f"C2 crop FAITHFUL vs FP32 oracle rel-L2 {e:.3e}")
     assert e <= FAITHFUL_TOL, e
+
+
+def test_c2_crop_half_storage_vs_fp64_oracle(c2crop):
+    """FP16 and BF16 volume storage at the C2 geometry (FP32 arithmetic; the
+    updates of each ordered subset are summed in FP32 and rounded to the
+    storage type once) against the FP64 oracle: FP16 within the 2e-3 bar,
+    BF16 (8 significant bits) within 1e-2."""
+    from oracle.parity import reconstruct_gpu
+
+    for vt, tol in (("f16", 2e-3), ("bf16", 1e-2)):
+        v = reconstruct_gpu(c2crop.workload, "fast", vt)
+        e = rel_l2(v, c2crop.oracle[1])
+        print(f"C2 crop FAST {vt} storage vs FP64 oracle rel-L2 {e:.3e}")
+        assert e <= tol, (vt, e)
