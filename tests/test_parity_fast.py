@@ -115,8 +115,11 @@ def test_fast_back_projection_exact_chords(case, os_, linear, slab):
         assert e <= 1e-5, (i, e)
 
 
-@pytest.mark.parametrize("sirt,os_", [(1, 1), (3, 2)])
-def test_fast_sart_volume(sirt, os_):
+@pytest.mark.parametrize("sirt,os_,aniso", [(1, 1, False), (3, 2, False), (2, 3, False), (3, 2, True)])
+def test_fast_sart_volume(sirt, os_, aniso):
+    """FAST SART against the oracle (FP32 1e-3, FP64 2e-4). Oversampling 3
+    and magnification anisotropy take the back-projector that filters the
+    residual itself (no pre-sampled images)."""
     import artiatomi_b200 as E
     from oracle.driver import OracleReconstructor
     from tests.test_parity_recon import _projections
@@ -127,13 +130,16 @@ def test_fast_sart_volume(sirt, os_):
     il = E.projection_index_list(E.PLT_RANDOM_START_ZERO_TILT, case["tilt"])
     cfgd = dict(lambda_=0.5, oversampling=os_, cut_length=(1.0, 1.0), dim_length=(3.0, 3.0),
                 crop=(1.0, 2.0, 1.0, 2.0), crop_dim=(3.0, 3.0, 3.0, 3.0))
+    m = mi = None
+    if aniso:
+        m, mi = E.mag_aniso_matrix(1.03, 25.0, W, H), E.mag_aniso_matrix(1.0 / 1.03, 25.0, W, H)
     rec = E.Reconstructor(E.ReconConfig(W, H, len(case["tilt"]), variant=E.VARIANT_FAST, **cfgd), case["pg"],
-                          case["tilt"])
+                          case["tilt"], None, m, mi)
     vol_d = cuda(np.zeros(case["vol"].shape, np.float32))
     rec.sart(case["vg"], vol_d, cuda(projs), il, iterations=2, sirt_count=sirt)
     got = host(vol_d)
     for prec, tol in ((0, 1e-3), (1, 2e-4)):
-        orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], precision=prec)
+        orc = OracleReconstructor(cfgd, W, H, case["og"], case["tilt"], aniso=m, aniso_inv=mi, precision=prec)
         vo = np.zeros(case["vol"].shape, np.float32)
         orc.sart(case["vo"], vo, 0, projs, il, 2, sirt)
         e = rel_l2(got, vo)
